@@ -1,0 +1,189 @@
+"""eafcg-b200: the EAF3D pressure-correction CG on NVIDIA B200 (sm_100a).
+
+The Python face of libeafcg.so. ``cg_3d`` mirrors the reference subroutine
+
+    cg_3d_mpi(aW, aE, aS, aN, aB, aT, aP, Su, phi, m, max_iter, tol,
+              residual, n_iter)            (src/mod_solver_3d.f90:485-496)
+
+argument for argument: the eight coefficient/RHS arrays and ``phi`` are FP64
+arrays in the reference workspace layout (Fortran (-1:nr+2,-1:nth+2,-1:nz+2),
+i.e. C-order numpy shape (nz+4, nth+4, nr+4)), ``phi`` is updated in place
+(interior plus theta-halo columns), and (residual, n_iter) is returned.
+As in the reference, a NaN residual is returned rather than raised
+(src/mod_pressure_3d.f90:322); every other failure raises EafError.
+
+All compute runs in the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import (EAF_EBUSY, EAF_ENONFINITE, EAF_ETIMEOUT, EAF_OK, EafError,
+                   check, load)
+
+SOR_TOL_PRESSURE = 1.0e-8     # src/mod_constants.f90:143
+MAX_INNER_PRES = 50           # src/mod_config_3d.f90:41 (default cap)
+
+__all__ = ["CGSolver", "cg_3d", "EafError", "load", "SOR_TOL_PRESSURE",
+           "MAX_INNER_PRES", "halo_shape"]
+
+
+def halo_shape(nr: int, nth: int, nz: int) -> tuple:
+    return (nz + 4, nth + 4, nr + 4)
+
+
+def _ptr(a) -> ctypes.c_void_p:
+    """Address of a numpy array (host) or of an object with data_ptr()."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("arrays must be C-contiguous float64")
+        return ctypes.c_void_p(a.ctypes.data)
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    if isinstance(a, int):
+        return ctypes.c_void_p(a)
+    raise TypeError(f"unsupported array type {type(a)!r}")
+
+
+class CGSolver:
+    """One mesh's solver handle (device mirrors and workspace on one GPU)."""
+
+    def __init__(self, nr: int, nth: int, nz: int, device: int = 0,
+                 is_parallel: bool = False):
+        self._lib = load()
+        self.nr, self.nth, self.nz, self.device = nr, nth, nz, device
+        h = ctypes.c_void_p()
+        check(self._lib.eaf_cg_create_mesh(ctypes.byref(h), nr, nth, nz,
+                                           int(bool(is_parallel)), device),
+              "eaf_cg_create")
+        self._h = h
+
+    @property
+    def ncells(self) -> int:
+        return self.nr * self.nth * self.nz
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.eaf_cg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check_shape(self, arrays) -> None:
+        shp = halo_shape(self.nr, self.nth, self.nz)
+        for a in arrays:
+            if isinstance(a, np.ndarray) and a.shape != shp:
+                raise ValueError(f"array shape {a.shape} != halo shape {shp}")
+
+    def solve(self, arrays, phi, max_iter: int = MAX_INNER_PRES,
+              tol: float = SOR_TOL_PRESSURE, device_ptrs: bool = False):
+        """Plain FP64 solve. ``arrays`` = (aW, aE, aS, aN, aB, aT, aP, Su).
+
+        Returns (residual, n_iter, status); status is EAF_OK or
+        EAF_ENONFINITE, anything else raises.
+        """
+        arrays = list(arrays)
+        self._check_shape(arrays + [phi])
+        res = ctypes.c_double()
+        nit = ctypes.c_int()
+        fn = (self._lib.eaf_cg_solve_f64_device if device_ptrs
+              else self._lib.eaf_cg_solve_f64)
+        st = fn(self._h, *[_ptr(a) for a in arrays], _ptr(phi), int(max_iter),
+                float(tol), ctypes.byref(res), ctypes.byref(nit))
+        check(st, "eaf_cg_solve_f64", allow=(EAF_OK, EAF_ENONFINITE))
+        return res.value, nit.value, st
+
+    def solve_mixed(self, arrays, phi, tol: float = SOR_TOL_PRESSURE,
+                    inner_tol: float = 0.1, max_outer: int = 200,
+                    max_inner: int = 100000, device_ptrs: bool = False):
+        """Mixed FP32/FP64 solve. Returns (residual, n_iter, n_outer, status)."""
+        arrays = list(arrays)
+        self._check_shape(arrays + [phi])
+        res = ctypes.c_double()
+        nit = ctypes.c_int()
+        nout = ctypes.c_int()
+        fn = (self._lib.eaf_cg_solve_mixed_device if device_ptrs
+              else self._lib.eaf_cg_solve_mixed)
+        st = fn(self._h, *[_ptr(a) for a in arrays], _ptr(phi), int(max_outer),
+                int(max_inner), float(tol), float(inner_tol), ctypes.byref(res),
+                ctypes.byref(nit), ctypes.byref(nout))
+        check(st, "eaf_cg_solve_mixed", allow=(EAF_OK, EAF_ENONFINITE))
+        return res.value, nit.value, nout.value, st
+
+    def set_launch(self, block: int = 0, grid: int = 0) -> None:
+        check(self._lib.eaf_cg_set_launch(self._h, block, grid), "set_launch")
+
+    def launch(self) -> tuple:
+        b, g = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.eaf_cg_get_launch(self._h, ctypes.byref(b), ctypes.byref(g)))
+        return b.value, g.value
+
+    def set_timeout_ms(self, ms: float) -> None:
+        check(self._lib.eaf_cg_set_timeout_ms(self._h, float(ms)), "set_timeout")
+
+    def last_timing(self) -> dict:
+        s, k = ctypes.c_double(), ctypes.c_double()
+        sym, nk = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.eaf_cg_last_timing(self._h, ctypes.byref(s), ctypes.byref(k),
+                                           ctypes.byref(sym), ctypes.byref(nk)))
+        return {"solve_ms": s.value, "kernel_ms": k.value, "symmetric": sym.value,
+                "kernels": nk.value, "e2e_ms": self._lib.eaf_cg_last_e2e_ms(self._h)}
+
+    @property
+    def stream(self) -> int:
+        return self._lib.eaf_cg_stream(self._h) or 0
+
+
+_solvers: dict = {}
+
+
+def cg_3d(aW, aE, aS, aN, aB, aT, aP, Su, phi, max_iter: int = MAX_INNER_PRES,
+          tol: float = SOR_TOL_PRESSURE, device: int = 0):
+    """Mirror of cg_3d_mpi for a serial mesh; phi is updated in place.
+
+    The mesh size is read from phi's halo shape; one cached solver handle
+    per (mesh, device) keeps its device workspace across calls, as the
+    reference's persistent workspace arrays do (src/mod_workspace.f90:120-144).
+    Returns (residual, n_iter).
+    """
+    if phi.ndim != 3:
+        raise ValueError("phi must be a 3-D halo-layout array")
+    nz, nth, nr = (s - 4 for s in phi.shape)
+    key = (nr, nth, nz, device)
+    if key not in _solvers:
+        _solvers[key] = CGSolver(nr, nth, nz, device)
+    res, nit, _ = _solvers[key].solve((aW, aE, aS, aN, aB, aT, aP, Su), phi,
+                                      max_iter, tol)
+    return res, nit
+
+
+def host_empty(shape, dtype=np.float64) -> np.ndarray:
+    """A numpy array over pinned (page-locked) host memory from the library."""
+    lib = load()
+    nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    p = ctypes.c_void_p()
+    check(lib.eaf_host_alloc(ctypes.byref(p), max(nbytes, 1)), "eaf_host_alloc")
+    buf = (ctypes.c_char * max(nbytes, 1)).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+    # keep the allocation alive with the array and free it with the array
+    import weakref
+    weakref.finalize(buf, lib.eaf_host_free, ctypes.c_void_p(p.value))
+    return arr
+
+
+def barrier_timeout_selftest(device: int = 0, timeout_ms: float = 20.0) -> int:
+    return load().eaf_selftest_barrier_timeout(device, float(timeout_ms))

@@ -1,0 +1,97 @@
+"""ctypes binding of libeafcg.so (the C ABI declared in include/eafcg.h).
+
+Loading fails loudly when the library has not been built: there is no CPU
+or PyTorch fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libeafcg.so")
+
+EAF_OK = 0
+EAF_ECUDA = 1
+EAF_EINVAL = 2
+EAF_ENONFINITE = 3
+EAF_ETIMEOUT = 4
+EAF_EUNSUPPORTED = 5
+EAF_ENOMEM = 6
+EAF_EADMIT = 7
+EAF_EBUSY = 8
+EAF_ECLOSED = 9
+
+STATUS_NAMES = {
+    0: "EAF_OK", 1: "EAF_ECUDA", 2: "EAF_EINVAL", 3: "EAF_ENONFINITE",
+    4: "EAF_ETIMEOUT", 5: "EAF_EUNSUPPORTED", 6: "EAF_ENOMEM", 7: "EAF_EADMIT",
+    8: "EAF_EBUSY", 9: "EAF_ECLOSED",
+}
+
+# (name, restype, argtypes) for every exported symbol of include/eafcg.h.
+_ci, _cd, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+_pi, _pd = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+_sz = ctypes.c_size_t
+_A8 = [_vp] * 8
+
+SIGNATURES = [
+    ("eaf_status_string", ctypes.c_char_p, [_ci]),
+    ("eaf_last_error", ctypes.c_char_p, []),
+    ("eaf_version", ctypes.c_char_p, []),
+    ("eaf_cg_create", _ci, [ctypes.POINTER(_vp), _ci, _ci, _ci, _ci]),
+    ("eaf_cg_create_mesh", _ci, [ctypes.POINTER(_vp), _ci, _ci, _ci, _ci, _ci]),
+    ("eaf_cg_destroy", _ci, [_vp]),
+    ("eaf_cg_solve_f64", _ci, [_vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
+    ("eaf_cg_solve_f64_device", _ci, [_vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
+    ("eaf_cg_solve_mixed", _ci,
+     [_vp] + _A8 + [_vp, _ci, _ci, _cd, _cd, _pd, _pi, _pi]),
+    ("eaf_cg_solve_mixed_device", _ci,
+     [_vp] + _A8 + [_vp, _ci, _ci, _cd, _cd, _pd, _pi, _pi]),
+    ("eaf_cg_set_launch", _ci, [_vp, _ci, _ci]),
+    ("eaf_cg_get_launch", _ci, [_vp, _pi, _pi]),
+    ("eaf_cg_set_timeout_ms", _ci, [_vp, _cd]),
+    ("eaf_cg_last_timing", _ci, [_vp, _pd, _pd, _pi, _pi]),
+    ("eaf_cg_last_e2e_ms", _cd, [_vp]),
+    ("eaf_cg_stream", _vp, [_vp]),
+    ("eaf_host_alloc", _ci, [ctypes.POINTER(_vp), _sz]),
+    ("eaf_host_free", _ci, [_vp]),
+    ("eaf_host_register", _ci, [_vp, _sz]),
+    ("eaf_host_unregister", _ci, [_vp]),
+    ("eaf_selftest_barrier_timeout", _ci, [_ci, _cd]),
+]
+
+_lib = None
+
+
+class EafError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        name = STATUS_NAMES.get(status, f"status {status}")
+        detail = ""
+        if status == EAF_ECUDA and _lib is not None:
+            detail = " (" + (_lib.eaf_last_error() or b"").decode() + ")"
+        super().__init__(f"{what}: {name}{detail}" if what else name + detail)
+
+
+def load() -> ctypes.CDLL:
+    """The loaded library; raises if it was never built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"libeafcg.so is missing at {LIB_PATH}; build it with "
+            "`python hornofusion-full3d_b200/build.py` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int, what: str = "", allow=(EAF_OK,)) -> int:
+    if status not in allow:
+        raise EafError(status, what)
+    return status

@@ -1,0 +1,496 @@
+// C-ABI shim of libeafcg.so: handle lifetime, device buffers, uploads,
+// launches, result readback and timing for the single-system solvers.
+// The public contract is documented in include/eafcg.h.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+
+#include "cg_kernels.h"
+#include "eafcg.h"
+#include "eafcg_internal.h"
+
+using eaf::GroupWs;
+using eaf::HaloInputs;
+using eaf::MeshDims;
+using eaf::SolveResult;
+using eaf::SysF32;
+using eaf::SysF64;
+
+namespace {
+
+constexpr int kPartSlots = 8;
+constexpr int kDefaultBlock = 512;
+constexpr uint64_t kDefaultTimeoutNs = 2000ull * 1000ull * 1000ull;
+
+}  // namespace
+
+struct eaf_cg {
+  int nr, nth, nz, device;
+  MeshDims d;
+  size_t nh;  // halo-layout elements per array
+  cudaStream_t st;
+  double* stage[9];  // aW aE aS aN aB aT aP Su phi, halo layout (host path)
+  SysF64 s;
+  SysF32 f;
+  bool have_f32;
+  GroupWs ws;
+  SolveResult* res_h;  // pinned
+  int block, grid;     // 0 = automatic
+  int sms;
+  uint64_t timeout_ns;
+  cudaEvent_t ev[6];   // e2e0, solve0, kern0, kern1, solve1, e2e1
+  double last_solve_ms, last_kernel_ms, last_e2e_ms;
+  int last_sym, last_kernels;
+};
+
+namespace eaf {
+
+thread_local char g_last_error[256];
+
+void set_error(const char* what, cudaError_t e) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s: %s", what,
+           e == cudaSuccess ? "ok" : cudaGetErrorString(e));
+}
+
+DeviceGuard::DeviceGuard(int dev) : prev_(-1), ok_(false) {
+  if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+  ok_ = cudaSetDevice(dev) == cudaSuccess;
+}
+DeviceGuard::~DeviceGuard() {
+  if (prev_ >= 0) cudaSetDevice(prev_);
+}
+
+}  // namespace eaf
+
+using eaf::set_error;
+
+#define EAF_CUDA(call)                     \
+  do {                                     \
+    cudaError_t e_ = (call);               \
+    if (e_ != cudaSuccess) {               \
+      set_error(#call, e_);                \
+      return EAF_ECUDA;                    \
+    }                                      \
+  } while (0)
+
+static void free_handle(eaf_cg* h) {
+  for (int i = 0; i < 9; ++i) cudaFree(h->stage[i]);
+  double* f64[] = {h->s.aP, h->s.aE, h->s.aN, h->s.aT, h->s.aW, h->s.aS,
+                   h->s.aB, h->s.b,  h->s.x,  h->s.r,  h->s.p,  h->s.q};
+  for (double* p : f64) cudaFree(p);
+  cudaFree(h->s.asym);
+  float* f32[] = {h->f.aP, h->f.aE, h->f.aN, h->f.aT, h->f.aW, h->f.aS, h->f.aB,
+                  h->f.r,  h->f.p,  h->f.q,  h->f.e};
+  for (float* p : f32) cudaFree(p);
+  cudaFree(h->ws.part);
+  cudaFree(h->ws.counter);
+  cudaFree(h->ws.err);
+  cudaFree(h->ws.result);
+  if (h->res_h) cudaFreeHost(h->res_h);
+  for (int i = 0; i < 6; ++i)
+    if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+  if (h->st) cudaStreamDestroy(h->st);
+}
+
+static int max_coresident(const void* kernel, int block, int sms) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) !=
+      cudaSuccess)
+    return 0;
+  return per_sm * sms;
+}
+
+// Launch shape for a persistent kernel over n cells.
+static void pick_launch(const eaf_cg* h, const void* kernel, int* grid, int* block) {
+  int b = h->block > 0 ? h->block : kDefaultBlock;
+  int cap = max_coresident(kernel, b, h->sms);
+  int g;
+  if (h->grid > 0) {
+    g = h->grid;
+  } else if (h->d.n <= 8192) {
+    b = h->block > 0 ? h->block : 1024;
+    cap = max_coresident(kernel, b, h->sms);
+    g = 1;
+  } else {
+    long long want = ((long long)h->d.n + (long long)b * 4 - 1) / ((long long)b * 4);
+    g = (int)(want < 1 ? 1 : want);
+  }
+  if (cap > 0 && g > cap) g = cap;
+  if (g > h->sms * 8) g = h->sms * 8;
+  *grid = g;
+  *block = b;
+}
+
+extern "C" {
+
+const char* eaf_status_string(int s) {
+  switch (s) {
+    case EAF_OK: return "EAF_OK";
+    case EAF_ECUDA: return "EAF_ECUDA";
+    case EAF_EINVAL: return "EAF_EINVAL";
+    case EAF_ENONFINITE: return "EAF_ENONFINITE";
+    case EAF_ETIMEOUT: return "EAF_ETIMEOUT";
+    case EAF_EUNSUPPORTED: return "EAF_EUNSUPPORTED";
+    case EAF_ENOMEM: return "EAF_ENOMEM";
+    case EAF_EADMIT: return "EAF_EADMIT";
+    case EAF_EBUSY: return "EAF_EBUSY";
+    case EAF_ECLOSED: return "EAF_ECLOSED";
+    default: return "EAF_UNKNOWN";
+  }
+}
+
+const char* eaf_last_error(void) { return eaf::g_last_error; }
+
+const char* eaf_version(void) { return "eafcg-b200 0.1 (sm_100a)"; }
+
+int eaf_cg_create_mesh(eaf_cg_t* out, int nr, int nth, int nz, int is_parallel,
+                       int device) {
+  if (!out) return EAF_EINVAL;
+  *out = nullptr;
+  if (is_parallel) return EAF_EUNSUPPORTED;
+  if (nr < 1 || nth < 1 || nz < 1) return EAF_EINVAL;
+  const long long n = (long long)nr * nth * nz;
+  const long long nh = (long long)(nr + 4) * (nth + 4) * (nz + 4);
+  if (nh >= (1ll << 31)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(device);
+  if (!guard.ok()) {
+    set_error("cudaSetDevice", cudaErrorInvalidDevice);
+    return EAF_ECUDA;
+  }
+  eaf_cg* h = new (std::nothrow) eaf_cg;
+  if (!h) return EAF_ENOMEM;
+  memset(h, 0, sizeof(*h));
+  h->nr = nr;
+  h->nth = nth;
+  h->nz = nz;
+  h->device = device;
+  h->d = eaf::make_dims(nr, nth, nz);
+  h->nh = (size_t)nh;
+  h->timeout_ns = kDefaultTimeoutNs;
+  int rc = EAF_OK;
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+  for (int i = 0; i < 9; ++i) alloc((void**)&h->stage[i], h->nh * sizeof(double));
+  double** f64[] = {&h->s.aP, &h->s.aE, &h->s.aN, &h->s.aT, &h->s.aW, &h->s.aS,
+                    &h->s.aB, &h->s.b,  &h->s.x,  &h->s.r,  &h->s.p,  &h->s.q};
+  for (double** p : f64) alloc((void**)p, (size_t)n * sizeof(double));
+  alloc((void**)&h->s.asym, sizeof(int));
+  int dev_sms = 0;
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
+  h->sms = dev_sms > 0 ? dev_sms : 148;
+  alloc((void**)&h->ws.part, sizeof(double) * kPartSlots * h->sms * 8);
+  alloc((void**)&h->ws.counter, sizeof(unsigned long long));
+  alloc((void**)&h->ws.err, sizeof(int));
+  alloc((void**)&h->ws.result, sizeof(SolveResult));
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&h->res_h, sizeof(SolveResult), 0);
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  if (e != cudaSuccess) {
+    set_error("eaf_cg_create", e);
+    rc = (e == cudaErrorMemoryAllocation) ? EAF_ENOMEM : EAF_ECUDA;
+    free_handle(h);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return EAF_OK;
+}
+
+int eaf_cg_create(eaf_cg_t* out, int nr, int nth, int nz, int device) {
+  return eaf_cg_create_mesh(out, nr, nth, nz, 0, device);
+}
+
+int eaf_cg_destroy(eaf_cg_t h) {
+  if (!h) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  cudaStreamSynchronize(h->st);
+  free_handle(h);
+  delete h;
+  return EAF_OK;
+}
+
+int eaf_cg_set_launch(eaf_cg_t h, int block_threads, int grid_blocks) {
+  if (!h || block_threads < 0 || grid_blocks < 0) return EAF_EINVAL;
+  if (block_threads != 0 &&
+      (block_threads % 32 != 0 || block_threads > 1024 || block_threads < 64))
+    return EAF_EINVAL;
+  h->block = block_threads;
+  h->grid = grid_blocks;
+  return EAF_OK;
+}
+
+int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks) {
+  if (!h || !block_threads || !grid_blocks) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  pick_launch(h, eaf::cg_f64_kernel_ptr(), grid_blocks, block_threads);
+  return EAF_OK;
+}
+
+int eaf_cg_set_timeout_ms(eaf_cg_t h, double ms) {
+  if (!h || !(ms > 0.0)) return EAF_EINVAL;
+  h->timeout_ns = (uint64_t)(ms * 1.0e6);
+  return EAF_OK;
+}
+
+int eaf_cg_last_timing(eaf_cg_t h, double* solve_ms, double* kernel_ms, int* sym,
+                       int* kernels) {
+  if (!h) return EAF_EINVAL;
+  if (solve_ms) *solve_ms = h->last_solve_ms;
+  if (kernel_ms) *kernel_ms = h->last_kernel_ms;
+  if (sym) *sym = h->last_sym;
+  if (kernels) *kernels = h->last_kernels;
+  return EAF_OK;
+}
+
+double eaf_cg_last_e2e_ms(eaf_cg_t h) { return h ? h->last_e2e_ms : 0.0; }
+
+void* eaf_cg_stream(eaf_cg_t h) { return h ? (void*)h->st : nullptr; }
+
+int eaf_host_alloc(void** ptr, size_t bytes) {
+  if (!ptr) return EAF_EINVAL;
+  cudaError_t e = cudaHostAlloc(ptr, bytes, cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    set_error("cudaHostAlloc", e);
+    return EAF_ENOMEM;
+  }
+  return EAF_OK;
+}
+int eaf_host_free(void* ptr) {
+  EAF_CUDA(cudaFreeHost(ptr));
+  return EAF_OK;
+}
+int eaf_host_register(void* ptr, size_t bytes) {
+  if (!ptr || !bytes) return EAF_EINVAL;
+  EAF_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterPortable));
+  return EAF_OK;
+}
+int eaf_host_unregister(void* ptr) {
+  if (!ptr) return EAF_EINVAL;
+  EAF_CUDA(cudaHostUnregister(ptr));
+  return EAF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Solve paths
+// ---------------------------------------------------------------------------
+namespace {
+
+bool any_null(const double* const* p, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!p[i]) return true;
+  return false;
+}
+
+int ensure_f32(eaf_cg* h) {
+  if (h->have_f32) return EAF_OK;
+  const size_t n = (size_t)h->d.n;
+  float** f32[] = {&h->f.aP, &h->f.aE, &h->f.aN, &h->f.aT, &h->f.aW, &h->f.aS,
+                   &h->f.aB, &h->f.r,  &h->f.p,  &h->f.q,  &h->f.e};
+  for (float** p : f32) {
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(float));
+    if (e != cudaSuccess) {
+      set_error("cudaMalloc(f32)", e);
+      return EAF_ENOMEM;
+    }
+  }
+  h->have_f32 = true;
+  return EAF_OK;
+}
+
+struct SolveOpts {
+  bool mixed;
+  int max_iter;   // plain: max_iter; mixed: max_inner
+  int max_outer;  // mixed only
+  double tol, inner_tol;
+};
+
+// Device-side solve: inputs in halo layout on the device, phi written in
+// place. Enqueues pack, solver, unpack on h->st; does not synchronise.
+int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts& o) {
+  EAF_CUDA(cudaEventRecord(h->ev[1], h->st));
+  EAF_CUDA(eaf::launch_pack_f64(h->d, in, h->s, h->st));
+  int grid, block;
+  if (o.mixed) {
+    int rc = ensure_f32(h);
+    if (rc != EAF_OK) return rc;
+    pick_launch(h, eaf::cg_mixed_kernel_ptr(), &grid, &block);
+    EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
+    EAF_CUDA(eaf::launch_cg_mixed(h->d, h->s, h->f, h->ws, o.max_outer, o.max_iter,
+                                  o.tol, o.inner_tol, h->timeout_ns, grid, block,
+                                  h->st));
+  } else {
+    pick_launch(h, eaf::cg_f64_kernel_ptr(), &grid, &block);
+    EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
+    EAF_CUDA(eaf::launch_cg_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
+                                grid, block, h->st));
+  }
+  EAF_CUDA(cudaEventRecord(h->ev[3], h->st));
+  EAF_CUDA(eaf::launch_unpack_f64(h->d, h->s.x, phi, h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[4], h->st));
+  EAF_CUDA(cudaMemcpyAsync(h->res_h, h->ws.result, sizeof(SolveResult),
+                           cudaMemcpyDeviceToHost, h->st));
+  h->last_kernels = 3;
+  return EAF_OK;
+}
+
+int finish_solve(eaf_cg* h, bool host_path, double* residual, int* n_iter,
+                 int* n_outer) {
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[1], h->ev[4]) == cudaSuccess) h->last_solve_ms = ms;
+  if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
+  if (host_path && cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]) == cudaSuccess)
+    h->last_e2e_ms = ms;
+  const SolveResult& r = *h->res_h;
+  h->last_sym = r.sym;
+  if (residual) *residual = r.residual;
+  if (n_iter) *n_iter = r.n_iter;
+  if (n_outer) *n_outer = r.n_outer;
+  return r.status;
+}
+
+int solve_device(eaf_cg* h, const double* const arr[8], double* phi,
+                 const SolveOpts& o, double* residual, int* n_iter, int* n_outer) {
+  if (!h || !phi || !residual || !n_iter || any_null(arr, 8)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  HaloInputs in = {arr[0], arr[1], arr[2], arr[3], arr[4], arr[5], arr[6], arr[7], phi};
+  int rc = enqueue_solve(h, in, phi, o);
+  if (rc != EAF_OK) return rc;
+  return finish_solve(h, false, residual, n_iter, n_outer);
+}
+
+int solve_host(eaf_cg* h, const double* const arr[8], double* phi, const SolveOpts& o,
+               double* residual, int* n_iter, int* n_outer) {
+  if (!h || !phi || !residual || !n_iter || any_null(arr, 8)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  const size_t bytes = h->nh * sizeof(double);
+  EAF_CUDA(cudaEventRecord(h->ev[0], h->st));
+  for (int i = 0; i < 8; ++i)
+    EAF_CUDA(cudaMemcpyAsync(h->stage[i], arr[i], bytes, cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(h->stage[8], phi, bytes, cudaMemcpyHostToDevice, h->st));
+  HaloInputs in = {h->stage[0], h->stage[1], h->stage[2], h->stage[3], h->stage[4],
+                   h->stage[5], h->stage[6], h->stage[7], h->stage[8]};
+  int rc = enqueue_solve(h, in, h->stage[8], o);
+  if (rc != EAF_OK) return rc;
+  EAF_CUDA(cudaMemcpyAsync(phi, h->stage[8], bytes, cudaMemcpyDeviceToHost, h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[5], h->st));
+  return finish_solve(h, true, residual, n_iter, n_outer);
+}
+
+}  // namespace
+
+extern "C" {
+
+int eaf_cg_solve_f64(eaf_cg_t h, const double* aW, const double* aE, const double* aS,
+                     const double* aN, const double* aB, const double* aT,
+                     const double* aP, const double* Su, double* phi, int max_iter,
+                     double tol, double* residual, int* n_iter) {
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  SolveOpts o = {false, max_iter, 0, tol, 0.0};
+  return solve_host(h, arr, phi, o, residual, n_iter, nullptr);
+}
+
+int eaf_cg_solve_f64_device(eaf_cg_t h, const double* aW, const double* aE,
+                            const double* aS, const double* aN, const double* aB,
+                            const double* aT, const double* aP, const double* Su,
+                            double* phi, int max_iter, double tol, double* residual,
+                            int* n_iter) {
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  SolveOpts o = {false, max_iter, 0, tol, 0.0};
+  return solve_device(h, arr, phi, o, residual, n_iter, nullptr);
+}
+
+int eaf_cg_solve_mixed(eaf_cg_t h, const double* aW, const double* aE, const double* aS,
+                       const double* aN, const double* aB, const double* aT,
+                       const double* aP, const double* Su, double* phi, int max_outer,
+                       int max_inner, double tol, double inner_tol, double* residual,
+                       int* n_iter, int* n_outer) {
+  if (!(inner_tol > 0.0 && inner_tol < 1.0) || max_inner < 1) return EAF_EINVAL;
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  SolveOpts o = {true, max_inner, max_outer, tol, inner_tol};
+  return solve_host(h, arr, phi, o, residual, n_iter, n_outer);
+}
+
+int eaf_cg_solve_mixed_device(eaf_cg_t h, const double* aW, const double* aE,
+                              const double* aS, const double* aN, const double* aB,
+                              const double* aT, const double* aP, const double* Su,
+                              double* phi, int max_outer, int max_inner, double tol,
+                              double inner_tol, double* residual, int* n_iter,
+                              int* n_outer) {
+  if (!(inner_tol > 0.0 && inner_tol < 1.0) || max_inner < 1) return EAF_EINVAL;
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  SolveOpts o = {true, max_inner, max_outer, tol, inner_tol};
+  return solve_device(h, arr, phi, o, residual, n_iter, n_outer);
+}
+
+// ---------------------------------------------------------------------------
+// Barrier self-test: two blocks wait on a counter that only reaches half of
+// its target, so every wait runs into its bound and the kernel reports
+// EAF_ETIMEOUT through the error word; the context stays usable.
+// ---------------------------------------------------------------------------
+int eaf_selftest_barrier_timeout(int device, double timeout_ms) {
+  if (!(timeout_ms > 0.0) || timeout_ms > 10000.0) return EAF_EINVAL;
+  eaf::DeviceGuard guard(device);
+  if (!guard.ok()) return EAF_ECUDA;
+  GroupWs ws = {};
+  cudaStream_t st = nullptr;
+  int err_h = 0;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ws.part, sizeof(double) * 16);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ws.counter, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ws.err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ws.result, sizeof(SolveResult));
+  if (e == cudaSuccess)
+    e = eaf::launch_barrier_selftest(ws, (uint64_t)(timeout_ms * 1.0e6), st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&err_h, ws.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(ws.part);
+  cudaFree(ws.counter);
+  cudaFree(ws.err);
+  cudaFree(ws.result);
+  if (st) cudaStreamDestroy(st);
+  if (e != cudaSuccess) {
+    set_error("selftest", e);
+    return EAF_ECUDA;
+  }
+  return err_h;
+}
+
+}  // extern "C"
+
+namespace eaf {
+namespace {
+// Two blocks; the group is declared with three members, so the arrival
+// target of the first barrier is never reached and both waits expire.
+__global__ void barrier_selftest_kernel(GroupWs ws, uint64_t timeout_ns) {
+  Group g;
+  g.counter = ws.counter;
+  g.err = ws.err;
+  g.part = ws.part;
+  g.nb = 3;
+  g.bid = blockIdx.x;
+  g.timeout_ns = timeout_ns;
+  g.epoch = 0;
+  group_barrier(g);
+}
+}  // namespace
+
+cudaError_t launch_barrier_selftest(const GroupWs& ws, uint64_t timeout_ns,
+                                    cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&ws, (void*)&timeout_ns};
+  return cudaLaunchCooperativeKernel((const void*)barrier_selftest_kernel, dim3(2),
+                                     dim3(64), args, 0, st);
+}
+}  // namespace eaf

@@ -1,0 +1,205 @@
+// Device building blocks shared by the pressure-CG kernels: mesh indexing in
+// the compact device layout, bounded-wait group barriers and deterministic
+// block/group reductions.
+//
+// Compact device layout (one system): interior cells only, flat index
+//   c = i + nr*(j + nth*k),  0 <= i < nr, 0 <= j < nth, 0 <= k < nz,
+// r fastest (the reference's column-major order without the halo ring).
+// theta neighbours wrap (src/mod_mpi_topology.f90:303-311); r and z
+// neighbours outside the mesh read as zero, which is what the reference's
+// Krylov vectors hold in their r/z halos (src/mod_solver_3d.f90:505-507,526).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "eafcg.h"
+
+namespace eaf {
+
+constexpr double kSmall = 1.0e-30;  // SMALL, src/mod_constants.f90:53
+
+// Unsigned division by a runtime divisor d >= 1 for numerators below 2^31:
+// q = (umulhi(n, m) + n) >> s with s = ceil(log2 d) and
+// m = floor(2^32 (2^s - d) / d) + 1 (the round-up multiplier method of
+// Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994).
+struct FastDiv {
+  uint32_t d, m, s;
+  __host__ __device__ FastDiv() : d(1), m(1), s(0) {}
+  __host__ explicit FastDiv(uint32_t div) : d(div) {
+    s = 0;
+    while ((1ull << s) < d) ++s;
+    m = (uint32_t)(((1ull << 32) * ((1ull << s) - d)) / d + 1);
+  }
+  __device__ __forceinline__ uint32_t div(uint32_t n) const {
+    return (__umulhi(n, m) + n) >> s;
+  }
+};
+
+struct MeshDims {
+  int nr, nth, nz;
+  int n;       // nr*nth*nz
+  int plane;   // nr*nth
+  FastDiv fd_nr, fd_nth;
+};
+
+__device__ __forceinline__ void cell_ijk(const MeshDims& d, int c, int& i, int& j,
+                                         int& k) {
+  uint32_t t = d.fd_nr.div((uint32_t)c);
+  i = c - (int)t * d.nr;
+  uint32_t kk = d.fd_nth.div(t);
+  j = (int)t - (int)kk * d.nth;
+  k = (int)kk;
+}
+
+// ---------------------------------------------------------------------------
+// Memory-model helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p,
+                                                    unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ int ld_volatile_i32(const int* p) {
+  return *(const volatile int*)p;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// Group barrier: `nb` co-resident blocks (a cooperative launch, or one lane
+// of a batched launch) meet on a 64-bit arrival counter that is zeroed
+// before the launch. Every wait is bounded by `timeout_ns` of global time;
+// on expiry the waiter records EAF_ETIMEOUT in the shared error word and all
+// waiters of the group leave. A group of one block only needs __syncthreads.
+// ---------------------------------------------------------------------------
+struct Group {
+  unsigned long long* counter;
+  int* err;
+  double* part;       // [slots][nb] block partials of this group
+  int nb;             // blocks in the group
+  int bid;            // this block's index in the group
+  uint64_t timeout_ns;
+  unsigned long long epoch;  // barriers passed (meaningful in thread 0)
+};
+
+__device__ __forceinline__ bool group_barrier(Group& g) {
+  __shared__ int s_ok;
+  if (g.nb == 1) {
+    __syncthreads();
+    return true;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    g.epoch += 1;
+    const unsigned long long target = g.epoch * (unsigned long long)g.nb;
+    __threadfence();
+    red_release_add_u64(g.counter, 1ull);
+    int ok = 1;
+    const uint64_t t0 = global_ns();
+    uint32_t spins = 0;
+    while (ld_acquire_u64(g.counter) < target) {
+      if (ld_volatile_i32(g.err) != 0) { ok = 0; break; }
+      if ((++spins & 63u) == 0 && global_ns() - t0 > g.timeout_ns) {
+        atomicCAS(g.err, 0, (int)EAF_ETIMEOUT);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions. The warp stage is an xor butterfly, the block
+// stage folds warp partials in warp order, and the group stage has warp 0 of
+// every block fold the `nb` block partials in the same fixed order, so every
+// block of the group obtains the bit-identical total (the exit tests and
+// step lengths of all blocks therefore agree).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_allsum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int NV, typename T>
+__device__ __forceinline__ void block_sum_to_thread0(T (&v)[NV]) {
+  __shared__ T s_w[NV][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int m = 0; m < NV; ++m) v[m] = warp_allsum(v[m]);
+  if (lane == 0) {
+#pragma unroll
+    for (int m = 0; m < NV; ++m) s_w[m][w] = v[m];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      T t = lane < nw ? s_w[m][lane] : T(0);
+      v[m] = warp_allsum(t);
+    }
+  }
+}
+
+// Group all-reduce of NV sums. Per-thread and in-block sums are carried in
+// T (FP32 for the mixed-precision inner solve, FP64 otherwise); block
+// partials go to slots [slot, slot+NV) of the group's FP64 partial table and
+// are folded in FP64. Returns false if the barrier gave up.
+template <int NV, typename T>
+__device__ __forceinline__ bool group_allsum(T (&v)[NV], Group& g, int slot) {
+  __shared__ double s_tot[NV];
+  block_sum_to_thread0<NV, T>(v);
+  if (g.nb == 1) {
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) s_tot[m] = (double)v[m];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < NV; ++m) v[m] = (T)s_tot[m];
+    __syncthreads();
+    return true;
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int m = 0; m < NV; ++m) g.part[(size_t)(slot + m) * g.nb + g.bid] = (double)v[m];
+  }
+  const bool ok = group_barrier(g);
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      const double* p = g.part + (size_t)(slot + m) * g.nb;
+      double s = 0.0;
+      for (int b = lane; b < g.nb; b += 32) s = s + __ldcg(p + b);
+      s = warp_allsum(s);
+      if (lane == 0) s_tot[m] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < NV; ++m) v[m] = (T)s_tot[m];
+  return ok;
+}
+
+__device__ __forceinline__ double guard_small(double v) { return v > kSmall ? v : kSmall; }
+__device__ __forceinline__ float guard_small(float v) {
+  return v > 1.0e-30f ? v : 1.0e-30f;
+}
+
+}  // namespace eaf

@@ -1,0 +1,312 @@
+// Plain FP64 Jacobi-preconditioned CG for the SIMPLE pressure correction:
+// a B200 restatement of cg_3d_mpi (src/mod_solver_3d.f90:485-620).
+//
+// Built with -fmad=false: every a*b+c below is rounded twice, as the
+// reference's default gfortran build computes it, so the stencil, the
+// updates and the preconditioner match the reference cell by cell and only
+// the association of the scalar dot products differs.
+//
+// One persistent cooperative launch runs the whole solve. Each block owns a
+// contiguous slice of cells (compact layout, cg_common.cuh) in every phase;
+// an iteration is three phases separated by group barriers:
+//   S0  q = A p, partial p.q                       -> all-reduce p.q
+//   S1  x += alpha p, r -= alpha q, partial r.r
+//       and r.z with z = r / max(|aP|, SMALL)      -> all-reduce (r.r, r.z)
+//   S2  p = z + beta p                             -> barrier
+// The scalar recurrences (alpha, beta, residual, exit tests) are evaluated
+// redundantly and bit-identically by every block.
+#include <math.h>
+
+#include "cg_kernels.h"
+#include "stencil.cuh"
+
+namespace eaf {
+
+MeshDims make_dims(int nr, int nth, int nz) {
+  MeshDims d;
+  d.nr = nr;
+  d.nth = nth;
+  d.nz = nz;
+  d.plane = nr * nth;
+  d.n = nr * nth * nz;
+  d.fd_nr = FastDiv((uint32_t)nr);
+  d.fd_nth = FastDiv((uint32_t)nth);
+  return d;
+}
+
+namespace {
+
+constexpr int kUnroll = 4;
+constexpr int kMaxBlock = 1024;
+
+struct CgArgs {
+  MeshDims d;
+  SysF64 s;
+  GroupWs ws;
+  int max_iter;
+  double tol;
+  uint64_t timeout_ns;
+};
+
+template <bool SYM>
+__device__ void cg_body(const CgArgs& a, Group& g) {
+  const MeshDims& d = a.d;
+  const SysF64& s = a.s;
+  const Slice own = own_slice(d.n, g.nb, g.bid);
+  const Coefs<double> A = coefs_of<double>(s.aP, s.aE, s.aN, s.aT, s.aW, s.aS, s.aB);
+  const double* __restrict__ aP = s.aP;
+  const double* __restrict__ b = s.b;
+  double* __restrict__ x = s.x;
+  double* __restrict__ r = s.r;
+  double* __restrict__ p = s.p;
+  double* __restrict__ q = s.q;
+#define EAF_OWN_CELLS(...) EAF_FOR_OWN(own, kUnroll, c, __VA_ARGS__)
+
+  // Preamble (src/mod_solver_3d.f90:515-530): ||Su||, z = r/max(|aP|,SMALL),
+  // pv = z, r.z and r.r in one pass.
+  double v3[3] = {0.0, 0.0, 0.0};
+  EAF_OWN_CELLS({
+    const double bv = b[c], rv = r[c];
+    const double z = rv / guard_small(fabs(aP[c]));
+    p[c] = z;
+    v3[0] = v3[0] + bv * bv;
+    v3[1] = v3[1] + rv * rv;
+    v3[2] = v3[2] + rv * z;
+  })
+  bool ok = group_allsum<3>(v3, g, 0);
+  const double bnorm = sqrt(v3[0]);
+  double residual = 0.0;
+  int n_iter = 0;
+  bool nan_fill = false;
+  if (ok && !(bnorm < kSmall)) {
+    double rz = v3[2];
+    residual = sqrt(v3[1]) / bnorm;
+    if (residual != residual && a.max_iter >= 1) nan_fill = true;
+    for (int iter = 1; iter <= a.max_iter && !nan_fill; ++iter) {
+      // S0: q = A p, p.q  (src/mod_solver_3d.f90:533-536)
+      double v1[1] = {0.0};
+      EAF_OWN_CELLS({
+        const double qv = apply_row<SYM, double>(d, A, p, c);
+        q[c] = qv;
+        v1[0] = v1[0] + p[c] * qv;
+      })
+      if (!(ok = group_allsum<1>(v1, g, 3))) break;
+      const double pq = v1[0];
+      if (fabs(pq) < kSmall) break;
+      const double alpha = rz / pq;
+      // S1: phi += alpha pv; r -= alpha q; r.r; z and r.z (:538-553)
+      double v2[2] = {0.0, 0.0};
+      EAF_OWN_CELLS({
+        const double pv = p[c], qv = q[c], dv = aP[c];
+        const double xv = x[c] + alpha * pv;
+        const double rv = r[c] - alpha * qv;
+        x[c] = xv;
+        r[c] = rv;
+        const double z = rv / guard_small(fabs(dv));
+        v2[0] = v2[0] + rv * rv;
+        v2[1] = v2[1] + rv * z;
+      })
+      if (!(ok = group_allsum<2>(v2, g, 4))) break;
+      residual = sqrt(v2[0]) / bnorm;
+      n_iter = iter;
+      if (residual < a.tol) break;
+      // Once the residual is NaN the reference iterates a fixed point: the
+      // next direction and every later iterate are NaN in every cell, and it
+      // runs to max_iter. Produce that outcome directly.
+      if (residual != residual && iter < a.max_iter) { nan_fill = true; break; }
+      const double beta = v2[1] / guard_small(rz);
+      rz = v2[1];
+      // S2: pv = z + beta pv (:556-558)
+      EAF_OWN_CELLS({
+        const double z = r[c] / guard_small(fabs(aP[c]));
+        p[c] = z + beta * p[c];
+      })
+      if (!(ok = group_barrier(g))) break;
+    }
+    if (nan_fill) {
+      const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+      EAF_OWN_CELLS({ x[c] = qnan; })
+      residual = qnan;
+      n_iter = a.max_iter;
+    }
+  }
+#undef EAF_OWN_CELLS
+  if (g.bid == 0 && threadIdx.x == 0) {
+    SolveResult* res = a.ws.result;
+    const int err = ld_volatile_i32(a.ws.err);
+    res->status = err != 0 ? err : (isfinite(residual) ? EAF_OK : EAF_ENONFINITE);
+    res->n_iter = n_iter;
+    res->n_outer = 0;
+    res->sym = SYM ? 1 : 0;
+    res->residual = residual;
+    res->bnorm = bnorm;
+  }
+}
+
+__global__ void __launch_bounds__(kMaxBlock) cg_f64_kernel(CgArgs a) {
+  Group g;
+  g.counter = a.ws.counter;
+  g.err = a.ws.err;
+  g.part = a.ws.part;
+  g.nb = gridDim.x;
+  g.bid = blockIdx.x;
+  g.timeout_ns = a.timeout_ns;
+  g.epoch = 0;
+  if (*a.s.asym == 0)
+    cg_body<true>(a, g);
+  else
+    cg_body<false>(a, g);
+}
+
+// ---------------------------------------------------------------------------
+// pack / unpack
+// ---------------------------------------------------------------------------
+struct PackArgs {
+  MeshDims d;
+  HaloInputs in;
+  SysF64 s;
+  long long hy, hz;  // halo strides of j and k
+};
+
+__global__ void pack_f64_kernel(PackArgs a) {
+  const MeshDims& d = a.d;
+  const HaloInputs& in = a.in;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_ijk(d, c, i, j, k);
+    const long long h = (long long)(i + 2) + a.hy * (j + 2) + a.hz * (k + 2);
+    const long long hs = j > 0 ? h - a.hy : h + (long long)(d.nth - 1) * a.hy;
+    const long long hn = j < d.nth - 1 ? h + a.hy : h - (long long)(d.nth - 1) * a.hy;
+    const double aW = in.aW[h], aE = in.aE[h], aS = in.aS[h], aN = in.aN[h];
+    const double aB = in.aB[h], aT = in.aT[h], aP = in.aP[h], su = in.Su[h];
+    a.s.aP[c] = aP;
+    a.s.aE[c] = aE;
+    a.s.aN[c] = aN;
+    a.s.aT[c] = aT;
+    a.s.aW[c] = aW;
+    a.s.aS[c] = aS;
+    a.s.aB[c] = aB;
+    a.s.b[c] = su;
+    // Symmetric-form test: every link equals its partner's, wall links are
+    // zero (compared by value; a NaN link selects the general form).
+    const bool sym = (aW == (i > 0 ? in.aE[h - 1] : 0.0)) &&
+                     (i < d.nr - 1 || aE == 0.0) && (aS == in.aN[hs]) &&
+                     (aB == (k > 0 ? in.aT[h - a.hz] : 0.0)) &&
+                     (k < d.nz - 1 || aT == 0.0);
+    if (!sym) atomicOr(a.s.asym, 1);
+    // r = Su - A*phi exactly as the reference's first matvec
+    // (src/mod_solver_3d.f90:510-513): theta-wrapped interior neighbours,
+    // r/z halo cells of phi as given.
+    const double xc = in.phi[h];
+    const double y = aP * xc - aW * in.phi[h - 1] - aE * in.phi[h + 1] -
+                     aS * in.phi[hs] - aN * in.phi[hn] - aB * in.phi[h - a.hz] -
+                     aT * in.phi[h + a.hz];
+    a.s.x[c] = xc;
+    a.s.r[c] = su - y;
+  }
+}
+
+struct UnpackArgs {
+  MeshDims d;
+  const double* x;
+  double* phi;
+  int hy;            // nr + 4
+  int hj;            // nth + 4
+  FastDiv fd_hy, fd_hj;
+  long long total;   // (nr+4)(nth+4)(nz+4)
+};
+
+// Source column of a theta-halo column j in the reference's sequential copy
+// x(:,0,:)=x(:,nth,:); x(:,-1,:)=x(:,nth-1,:); x(:,nth+1,:)=x(:,1,:);
+// x(:,nth+2,:)=x(:,2,:) (src/mod_mpi_topology.f90:303-311), resolved to an
+// interior column (only differs from the plain rule when nth < 2).
+__device__ __forceinline__ int theta_source(int j, int nth) {
+  if (j == 0) return nth;
+  if (j == -1) return nth - 1 >= 1 ? nth - 1 : nth;
+  if (j == nth + 1) return 1;
+  return 2 <= nth ? 2 : 1;  // j == nth + 2
+}
+
+__global__ void unpack_f64_kernel(UnpackArgs a) {
+  const MeshDims& d = a.d;
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < a.total;
+       h += (long long)gridDim.x * blockDim.x) {
+    // halo coordinates -> Fortran indices
+    const uint32_t t = a.fd_hy.div((uint32_t)h);
+    const int i = (int)(h - (long long)t * a.hy) - 1;
+    const uint32_t kk = a.fd_hj.div(t);
+    const int j = (int)(t - kk * a.hj) - 1;
+    const int k = (int)kk - 1;
+    const bool iin = i >= 1 && i <= d.nr, kin = k >= 1 && k <= d.nz;
+    const bool jin = j >= 1 && j <= d.nth;
+    if (jin) {
+      if (iin && kin) a.phi[h] = a.x[(i - 1) + d.nr * ((j - 1) + d.nth * (k - 1))];
+    } else {
+      const int js = theta_source(j, d.nth);
+      if (iin && kin)
+        a.phi[h] = a.x[(i - 1) + d.nr * ((js - 1) + d.nth * (k - 1))];
+      else
+        a.phi[h] = a.phi[h + (long long)(js - j) * a.hy];
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_pack_f64(const MeshDims& d, const HaloInputs& in, const SysF64& s,
+                            cudaStream_t st) {
+  PackArgs a;
+  a.d = d;
+  a.in = in;
+  a.s = s;
+  a.hy = d.nr + 4;
+  a.hz = (long long)(d.nr + 4) * (d.nth + 4);
+  cudaError_t e = cudaMemsetAsync(s.asym, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int block = 256;
+  int grid = (d.n + block - 1) / block;
+  if (grid > 148 * 16) grid = 148 * 16;
+  pack_f64_kernel<<<grid, block, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_f64(const MeshDims& d, const double* x, double* phi,
+                              cudaStream_t st) {
+  UnpackArgs a;
+  a.d = d;
+  a.x = x;
+  a.phi = phi;
+  a.hy = d.nr + 4;
+  a.hj = d.nth + 4;
+  a.fd_hy = FastDiv((uint32_t)a.hy);
+  a.fd_hj = FastDiv((uint32_t)a.hj);
+  a.total = (long long)(d.nr + 4) * (d.nth + 4) * (d.nz + 4);
+  const int block = 256;
+  long long g = (a.total + block - 1) / block;
+  int grid = (int)(g > 148 * 16 ? 148 * 16 : g);
+  unpack_f64_kernel<<<grid, block, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                          int max_iter, double tol, uint64_t timeout_ns, int grid,
+                          int block, cudaStream_t st) {
+  CgArgs a;
+  a.d = d;
+  a.s = s;
+  a.ws = ws;
+  a.max_iter = max_iter;
+  a.tol = tol;
+  a.timeout_ns = timeout_ns;
+  cudaError_t e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  void* args[] = {&a};
+  return cudaLaunchCooperativeKernel((const void*)cg_f64_kernel, dim3(grid),
+                                     dim3(block), args, 0, st);
+}
+
+const void* cg_f64_kernel_ptr() { return (const void*)cg_f64_kernel; }
+
+}  // namespace eaf

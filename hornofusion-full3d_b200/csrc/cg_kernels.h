@@ -1,0 +1,84 @@
+// Internal launch interface between the C-ABI shim (api.cu) and the kernel
+// translation units. Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cg_common.cuh"
+
+namespace eaf {
+
+// Written by the solver kernel (block 0, thread 0) at the end of a solve.
+struct SolveResult {
+  int status;      // EAF_OK, EAF_ENONFINITE or EAF_ETIMEOUT
+  int n_iter;      // CG iterations (mixed form: total inner iterations)
+  int n_outer;     // refinement steps (mixed form), 0 for the plain form
+  int sym;         // 1 = symmetric 4-array operator, 0 = general 7-array
+  double residual; // final relative residual
+  double bnorm;    // ||Su||
+};
+
+// Halo-layout inputs of one solve (the reference workspace arrays).
+struct HaloInputs {
+  const double* aW;
+  const double* aE;
+  const double* aS;
+  const double* aN;
+  const double* aB;
+  const double* aT;
+  const double* aP;
+  const double* Su;
+  const double* phi;
+};
+
+// Compact-layout device state of one system (interior cells only).
+struct SysF64 {
+  double *aP, *aE, *aN, *aT;  // symmetric form: aW, aS, aB are implied
+  double *aW, *aS, *aB;       // general form only
+  double *b, *x, *r, *p, *q;
+  int* asym;                  // pack: number of link pairs that disagree
+};
+
+// FP32 shadow of a system for the mixed-precision inner solve.
+struct SysF32 {
+  float *aP, *aE, *aN, *aT, *aW, *aS, *aB;
+  float *r, *p, *q, *e;  // inner residual, direction, A p, correction
+};
+
+struct GroupWs {
+  double* part;                 // block partials, [slots][blocks]
+  unsigned long long* counter;  // barrier arrival counter (zeroed per launch)
+  int* err;                     // shared error word (zeroed per launch)
+  SolveResult* result;
+};
+
+MeshDims make_dims(int nr, int nth, int nz);
+
+// pack: halo layout -> compact layout, symmetry check, FP64 initial
+// residual r = Su - A phi with the reference stencil (phi's theta halo
+// wrapped, its r/z halo cells read as given).
+cudaError_t launch_pack_f64(const MeshDims& d, const HaloInputs& in,
+                            const SysF64& s, cudaStream_t st);
+// unpack: compact x -> phi interior + theta-halo columns over the full i, k
+// halo ranges (phi's r/z halo cells are left as they are).
+cudaError_t launch_unpack_f64(const MeshDims& d, const double* x, double* phi,
+                              cudaStream_t st);
+// Persistent cooperative plain-FP64 Jacobi-PCG.
+cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                          int max_iter, double tol, uint64_t timeout_ns,
+                          int grid, int block, cudaStream_t st);
+const void* cg_f64_kernel_ptr();
+
+// Mixed precision (cg_mixed.cu).
+cudaError_t launch_cg_mixed(const MeshDims& d, const SysF64& s, const SysF32& f,
+                            const GroupWs& ws, int max_outer, int max_inner,
+                            double tol, double inner_tol, uint64_t timeout_ns,
+                            int grid, int block, cudaStream_t st);
+const void* cg_mixed_kernel_ptr();
+
+// Barrier self-test (api.cu).
+cudaError_t launch_barrier_selftest(const GroupWs& ws, uint64_t timeout_ns,
+                                    cudaStream_t st);
+
+}  // namespace eaf

@@ -1,0 +1,271 @@
+"""Seeded synthetic pressure-correction systems (the ``eafgen`` generator).
+
+Builds the 7-point finite-volume Poisson operator that the SIMPLE pressure
+correction hands to its CG, on a uniform cylindrical (r, theta, z) mesh:
+
+* uniform dr = R/nr, dtheta = 2*pi/nth, dz = H/nz; r-centre (i - 1/2) dr;
+* face areas A_r = r_face dtheta dz (zero on the axis), A_theta = dr dz,
+  A_z = r dr dtheta -- the uniform-spacing form of the reference mesh metrics
+  (src/mod_mesh_3d.f90:125-156);
+* per-cell density: liquid steel 7000 kg/m3 where z < 0.6 m and r < 2.5 m,
+  gas 0.3 kg/m3 elsewhere, plus seeded scrap spheres at 7800 kg/m3;
+* per-cell momentum diagonal abar_P, log-uniform in [1e2, 1e4];
+* face link a_f = rho_f A_f^2 / abar_f with harmonic-mean rho_f and abar_f;
+* a_P = sum of the six links (W, E, S, N, B, T, in that order);
+* no-flux walls at r = R, z = 0 and z = H (links zeroed), periodic in theta;
+* cell (nr, 1, 1) pinned to p' = 0 and folded symmetrically the way
+  apply_pressure_bc folds its Dirichlet outlets (src/mod_boundary_3d.f90:
+  235-242, 263-270): its row becomes the identity with zero source, the links
+  of its neighbours into it are zeroed, and their a_P keep the term;
+* RHS b ~ N(0, 1e-3) with the mean over the free cells removed, b = 0 at the
+  pin; x0 = 0.
+
+Arrays come out in the reference workspace layout (src/mod_workspace.f90:
+24-27): Fortran ``(-1:nr+2, -1:nth+2, -1:nz+2)`` column-major with r fastest,
+which is a C-order numpy array of shape ``(nz+4, nth+4, nr+4)``. Halo entries
+are zero, as the reference assembler leaves them.
+
+Re-solves (the SIMPLE-like sequence) perturb abar_P by a fresh per-cell factor
+U[0.9, 1.1] of the base field, draw a fresh zero-mean RHS and are meant to be
+warm-started from the previous solution.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+R_FURNACE = 3.8
+H_FURNACE = 4.5
+RHO_STEEL = 7000.0
+RHO_GAS = 0.3
+RHO_SCRAP = 7800.0
+BATH_DEPTH = 0.6
+BATH_RADIUS = 2.5
+
+# Named workloads (mesh nr, nth, nz and scrap-sphere count).
+SMOKE = (12, 24, 16, 8)          # 4,608 cells
+PRODUCTION = (60, 120, 84, 24)   # 604,800 cells
+FINE = (120, 240, 168, 64)       # 4,838,400 cells
+BATCH_MIX = [((12, 24, 16, 8), 40), ((18, 36, 24, 8), 30),
+             ((35, 70, 50, 16), 20), ((60, 120, 84, 24), 6)]
+SERVE_MIX = [((18, 36, 24, 8), 0.50), ((35, 70, 50, 16), 0.35),
+             ((60, 120, 84, 24), 0.15)]
+
+COEF_NAMES = ("aW", "aE", "aS", "aN", "aB", "aT", "aP", "Su")
+
+
+def halo_shape(nr: int, nth: int, nz: int) -> tuple:
+    return (nz + 4, nth + 4, nr + 4)
+
+
+def interior(a: np.ndarray) -> np.ndarray:
+    """View of the interior cells 1..n of a halo-layout array."""
+    return a[2:-2, 2:-2, 2:-2]
+
+
+@dataclasses.dataclass
+class Mesh:
+    nr: int
+    nth: int
+    nz: int
+    nsph: int
+    seed: int
+    rho: np.ndarray      # (nz, nth, nr) cell density
+    abar: np.ndarray     # (nz, nth, nr) base momentum diagonal
+
+    @property
+    def ncells(self) -> int:
+        return self.nr * self.nth * self.nz
+
+
+@dataclasses.dataclass
+class System:
+    """One pressure-correction system in the reference halo layout."""
+    nr: int
+    nth: int
+    nz: int
+    aW: np.ndarray
+    aE: np.ndarray
+    aS: np.ndarray
+    aN: np.ndarray
+    aB: np.ndarray
+    aT: np.ndarray
+    aP: np.ndarray
+    Su: np.ndarray
+
+    @property
+    def ncells(self) -> int:
+        return self.nr * self.nth * self.nz
+
+    def arrays(self):
+        return [getattr(self, n) for n in COEF_NAMES]
+
+
+def _hmean(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    return 2.0 * a * b / (a + b)
+
+
+def make_mesh(nr: int, nth: int, nz: int, nsph: int, seed: int) -> Mesh:
+    """Density and base abar_P fields; draws spheres first, then abar_P."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dr = R_FURNACE / nr
+    dth = 2.0 * math.pi / nth
+    dz = H_FURNACE / nz
+    rc = (np.arange(nr) + 0.5) * dr
+    thc = (np.arange(nth) + 0.5) * dth
+    zc = (np.arange(nz) + 0.5) * dz
+    Z, TH, RR = np.meshgrid(zc, thc, rc, indexing="ij")
+    rho = np.where((Z < BATH_DEPTH) & (RR < BATH_RADIUS), RHO_STEEL, RHO_GAS)
+    u = rng.random((nsph, 4))
+    X = RR * np.cos(TH)
+    Y = RR * np.sin(TH)
+    for s in range(nsph):
+        rs = R_FURNACE * math.sqrt(u[s, 0])
+        ts = 2.0 * math.pi * u[s, 1]
+        zs = H_FURNACE * u[s, 2]
+        rad = 0.2 + 0.3 * u[s, 3]
+        xs, ys = rs * math.cos(ts), rs * math.sin(ts)
+        inside = (X - xs) ** 2 + (Y - ys) ** 2 + (Z - zs) ** 2 <= rad * rad
+        rho = np.where(inside, RHO_SCRAP, rho)
+    abar = np.exp(rng.uniform(math.log(1e2), math.log(1e4), size=(nz, nth, nr)))
+    return Mesh(nr, nth, nz, nsph, seed, rho.astype(np.float64), abar)
+
+
+def assemble(mesh: Mesh, abar: np.ndarray, b: np.ndarray) -> System:
+    """Face links, diagonal, pin fold and embedding into the halo layout."""
+    nr, nth, nz = mesh.nr, mesh.nth, mesh.nz
+    dr = R_FURNACE / nr
+    dth = 2.0 * math.pi / nth
+    dz = H_FURNACE / nz
+    rc = (np.arange(nr) + 0.5) * dr
+    rface = (np.arange(nr) + 1.0) * dr          # outer r face of cell i
+    rho = mesh.rho
+
+    aE = np.zeros((nz, nth, nr))
+    if nr > 1:
+        Ar = (rface[:-1] * dth * dz)[None, None, :]
+        aE[:, :, :-1] = (_hmean(rho[:, :, :-1], rho[:, :, 1:]) * Ar * Ar
+                         / _hmean(abar[:, :, :-1], abar[:, :, 1:]))
+    aW = np.zeros_like(aE)
+    aW[:, :, 1:] = aE[:, :, :-1]
+
+    Ath = dr * dz
+    rho_n = np.roll(rho, -1, axis=1)
+    abar_n = np.roll(abar, -1, axis=1)
+    aN = _hmean(rho, rho_n) * Ath * Ath / _hmean(abar, abar_n)
+    aS = np.roll(aN, 1, axis=1)
+
+    aT = np.zeros_like(aE)
+    if nz > 1:
+        Az = (rc * dr * dth)[None, None, :]
+        aT[:-1] = (_hmean(rho[:-1], rho[1:]) * Az * Az
+                   / _hmean(abar[:-1], abar[1:]))
+    aB = np.zeros_like(aE)
+    aB[1:] = aT[:-1]
+
+    aP = ((((aW + aE) + aS) + aN) + aB) + aT
+    Su = b.copy()
+
+    # Pin at Fortran (nr, 1, 1) = numpy [0, 0, nr-1]; fold its links.
+    pk, pj, pi = 0, 0, nr - 1
+    for arr in (aW, aE, aS, aN, aB, aT):
+        arr[pk, pj, pi] = 0.0
+    aP[pk, pj, pi] = 1.0
+    Su[pk, pj, pi] = 0.0
+    if nr > 1:
+        aE[pk, pj, pi - 1] = 0.0
+    aN[pk, (pj - 1) % nth, pi] = 0.0
+    aS[pk, (pj + 1) % nth, pi] = 0.0
+    if nz > 1:
+        aB[pk + 1, pj, pi] = 0.0
+
+    out = {}
+    for name, arr in zip(COEF_NAMES, (aW, aE, aS, aN, aB, aT, aP, Su)):
+        h = np.zeros(halo_shape(nr, nth, nz))
+        interior(h)[...] = arr
+        out[name] = h
+    return System(nr, nth, nz, **out)
+
+
+def draw_rhs(rng: np.random.Generator, nr: int, nth: int, nz: int) -> np.ndarray:
+    b = rng.normal(0.0, 1e-3, size=(nz, nth, nr))
+    free = np.ones_like(b, dtype=bool)
+    free[0, 0, nr - 1] = False
+    b[free] -= b[free].mean()
+    b[0, 0, nr - 1] = 0.0
+    return b
+
+
+def make_system(nr: int, nth: int, nz: int, nsph: int = 8, seed: int = 0,
+                resolve: int | None = None, mesh: Mesh | None = None) -> System:
+    """System ``resolve`` of the seeded sequence (None = the base system).
+
+    The base system uses the base abar_P field; re-solve s multiplies it by a
+    fresh per-cell U[0.9, 1.1] factor. Each has its own zero-mean RHS.
+    """
+    if mesh is None:
+        mesh = make_mesh(nr, nth, nz, nsph, seed)
+    if resolve is None:
+        rng = np.random.Generator(np.random.PCG64([seed, 1]))
+        abar = mesh.abar
+    else:
+        rng = np.random.Generator(np.random.PCG64([seed, 2, resolve]))
+        abar = mesh.abar * rng.uniform(0.9, 1.1, size=mesh.abar.shape)
+    b = draw_rhs(rng, nr, nth, nz)
+    return assemble(mesh, abar, b)
+
+
+def zeros_phi(nr: int, nth: int, nz: int) -> np.ndarray:
+    return np.zeros(halo_shape(nr, nth, nz))
+
+
+def make_known_answer(nr: int, nth: int, nz: int, nsph: int = 8,
+                      seed: int = 0):
+    """(system, x_star): the base operator with Su replaced by A x_star.
+
+    x_star is a smooth field (zero at the pin), so the solve has a known
+    answer that does not depend on any CG implementation.
+    """
+    sys_ = make_system(nr, nth, nz, nsph, seed)
+    dth = 2.0 * math.pi / nth
+    k = np.arange(nz)[:, None, None]
+    j = np.arange(nth)[None, :, None]
+    i = np.arange(nr)[None, None, :]
+    xs = (np.cos((j + 0.5) * dth) * (1.0 + 0.1 * i)
+          + 0.05 * np.sin(0.3 * k + 0.2 * i))
+    xs = np.broadcast_to(xs, (nz, nth, nr)).copy()
+    xs[0, 0, nr - 1] = 0.0
+    x_h = zeros_phi(nr, nth, nz)
+    interior(x_h)[...] = xs
+    interior(sys_.Su)[...] = apply_operator(sys_, x_h)
+    return sys_, x_h
+
+
+def apply_operator(s: System, x_h: np.ndarray) -> np.ndarray:
+    """y = A x on the interior (numpy, vectorised; theta wrapped, r/z halos
+    read as stored). Same expression order as the reference matvec
+    (src/mod_solver_3d.f90:595-603)."""
+    x = x_h.copy()
+    # theta-periodic halo fill (src/mod_mpi_topology.f90:303-311)
+    x[:, 1, :] = x[:, -3, :]
+    x[:, 0, :] = x[:, -4, :]
+    x[:, -2, :] = x[:, 2, :]
+    x[:, -1, :] = x[:, 3, :]
+    c = (slice(2, -2),) * 3
+    xc = x[c]
+    xw = x[2:-2, 2:-2, 1:-3]
+    xe = x[2:-2, 2:-2, 3:-1]
+    xs = x[2:-2, 1:-3, 2:-2]
+    xn = x[2:-2, 3:-1, 2:-2]
+    xb = x[1:-3, 2:-2, 2:-2]
+    xt = x[3:-1, 2:-2, 2:-2]
+    I = interior
+    return (I(s.aP) * xc - I(s.aW) * xw - I(s.aE) * xe - I(s.aS) * xs
+            - I(s.aN) * xn - I(s.aB) * xb - I(s.aT) * xt)
+
+
+def system_bytes(nr: int, nth: int, nz: int) -> int:
+    """Host bytes of one system (8 halo-layout FP64 arrays)."""
+    return 8 * 8 * (nr + 4) * (nth + 4) * (nz + 4)

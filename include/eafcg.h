@@ -1,0 +1,164 @@
+/*
+ * eafcg.h -- C ABI of the B200 pressure-correction CG (libeafcg.so).
+ *
+ * Drop-in for the reference Jacobi-preconditioned CG
+ *   subroutine cg_3d_mpi(aW, aE, aS, aN, aB, aT, aP, Su, phi, m,
+ *                        max_iter, tol, residual, n_iter)
+ *   (src/mod_solver_3d.f90:485-496), called once per SIMPLE outer iteration
+ *   from solve_pressure_correction (src/mod_pressure_3d.f90:316-318).
+ *
+ * Array contract (every coefficient, Su and phi):
+ *   Fortran real(dp) (-1:nr+2, -1:nth+2, -1:nz+2), column-major, r fastest;
+ *   the pointer is element (-1,-1,-1); Fortran (i,j,k) sits at linear index
+ *   (i+1) + (nr+4)*((j+1) + (nth+4)*(k+1)).  This is the reference
+ *   workspace layout (src/mod_workspace.f90:24-27, src/mod_fields_3d.f90:265).
+ * Reads the interior of the coefficients and Su, and phi's interior plus its
+ * r/z halo cells that the 7-point stencil touches (the reference's first
+ * matvec reads them); writes phi's interior and its four theta-halo columns
+ * j = -1, 0, nth+1, nth+2 over the full i and k halo ranges, which is the
+ * serial theta-periodic copy the reference applies before returning
+ * (src/mod_solver_3d.f90:567, src/mod_mpi_topology.f90:303-311).
+ *
+ * Semantics follow cg_3d_mpi: relative residual ||r||/||Su|| with strict
+ * `< tol` exit after the update; Jacobi z = r / max(|aP|, 1e-30);
+ * breakdown exit when |p.q| < 1e-30; zero right-hand side (||Su|| < 1e-30)
+ * returns residual 0 and n_iter 0 with phi's interior untouched. Not
+ * reaching tol within max_iter is not an error. Scalar dots are reduced
+ * on the device in a fixed order, so results are reproducible run to run
+ * but not bit-identical to the reference's sequential sums.
+ *
+ * Every call is synchronous with respect to the host unless its name ends
+ * in _async. One handle must not be used by two host threads at once.
+ * The calling thread's current CUDA device is left as it was.
+ */
+#ifndef EAFCG_H
+#define EAFCG_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum eaf_status {
+  EAF_OK = 0,
+  EAF_ECUDA = 1,         /* a CUDA runtime call failed                     */
+  EAF_EINVAL = 2,        /* bad argument (NULL pointer, size, tolerance)   */
+  EAF_ENONFINITE = 3,    /* the residual came out NaN or Inf; it is still
+                            returned (the caller propagates NaN, as
+                            src/mod_pressure_3d.f90:322 does)              */
+  EAF_ETIMEOUT = 4,      /* a bounded device or queue wait gave up         */
+  EAF_EUNSUPPORTED = 5,  /* e.g. a decomposed (is_parallel) mesh           */
+  EAF_ENOMEM = 6,        /* device or host allocation failed               */
+  EAF_EADMIT = 7,        /* serving: run refused by the HBM budget         */
+  EAF_EBUSY = 8,         /* serving: result not ready yet                  */
+  EAF_ECLOSED = 9        /* serving: server shut down / run closed         */
+};
+
+/* Human-readable name of a status code (static storage). */
+const char* eaf_status_string(int status);
+
+/* Text of the last CUDA failure seen by this host thread. */
+const char* eaf_last_error(void);
+
+/* ---- single-system plain FP64 solver ----------------------------------- */
+typedef struct eaf_cg* eaf_cg_t;
+
+/* Creates a solver for one nr x nth x nz mesh on `device` (the whole theta x z
+ * domain on one GPU). Allocates all device mirrors and Krylov workspace once;
+ * replaces the per-call allocate/deallocate of r, z, pv, q
+ * (src/mod_solver_3d.f90:505-507, 569). */
+int eaf_cg_create(eaf_cg_t* out, int nr, int nth, int nz, int device);
+
+/* Same, for a caller that still holds a decomposed mesh: is_parallel != 0
+ * returns EAF_EUNSUPPORTED (there is no CPU fallback). Mirrors the
+ * m%is_parallel switch of cg_3d_mpi's bounds() (src/mod_solver_3d.f90:574-586). */
+int eaf_cg_create_mesh(eaf_cg_t* out, int nr, int nth, int nz, int is_parallel,
+                       int device);
+
+int eaf_cg_destroy(eaf_cg_t h);
+
+/* The drop-in: host arrays in the reference layout (pinned memory is
+ * faster but not required). Replaces the call at
+ * src/mod_pressure_3d.f90:316-318; argument meaning as
+ * src/mod_solver_3d.f90:485-496. */
+int eaf_cg_solve_f64(eaf_cg_t h, const double* aW, const double* aE,
+                     const double* aS, const double* aN, const double* aB,
+                     const double* aT, const double* aP, const double* Su,
+                     double* phi, int max_iter, double tol, double* residual,
+                     int* n_iter);
+
+/* Same contract with device pointers (same layout, on the handle's device).
+ * Inputs are read and phi is written on the handle's stream. */
+int eaf_cg_solve_f64_device(eaf_cg_t h, const double* aW, const double* aE,
+                            const double* aS, const double* aN, const double* aB,
+                            const double* aT, const double* aP, const double* Su,
+                            double* phi, int max_iter, double tol,
+                            double* residual, int* n_iter);
+
+/* Mixed precision: FP32 Jacobi-PCG inner solves (FP32 coefficients, vectors
+ * and dot accumulation) inside an FP64 iterative-refinement loop that keeps
+ * Su, phi, the outer residual Su - A phi, the convergence norm and the pin
+ * in FP64. Stops when ||Su - A phi|| / ||Su|| < tol or after max_outer
+ * refinement steps; each inner solve stops at relative reduction inner_tol
+ * or after max_inner iterations. n_iter returns the total inner iterations,
+ * n_outer the refinement steps. No reference counterpart: this is a new
+ * solver form behind the same array contract as eaf_cg_solve_f64. */
+int eaf_cg_solve_mixed(eaf_cg_t h, const double* aW, const double* aE,
+                       const double* aS, const double* aN, const double* aB,
+                       const double* aT, const double* aP, const double* Su,
+                       double* phi, int max_outer, int max_inner, double tol,
+                       double inner_tol, double* residual, int* n_iter,
+                       int* n_outer);
+int eaf_cg_solve_mixed_device(eaf_cg_t h, const double* aW, const double* aE,
+                              const double* aS, const double* aN,
+                              const double* aB, const double* aT,
+                              const double* aP, const double* Su, double* phi,
+                              int max_outer, int max_inner, double tol,
+                              double inner_tol, double* residual, int* n_iter,
+                              int* n_outer);
+
+/* Launch shape of the persistent kernel: threads per block and number of
+ * co-resident blocks (0 = automatic). Used by the autotuner. */
+int eaf_cg_set_launch(eaf_cg_t h, int block_threads, int grid_blocks);
+int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks);
+
+/* Bound on every device-side barrier wait, in milliseconds (default 2000). */
+int eaf_cg_set_timeout_ms(eaf_cg_t h, double ms);
+
+/* Device time of the last solve (pack + solve + unpack) and of its solver
+ * kernel alone, in milliseconds; 1 if the matrix was taken in the symmetric
+ * 4-array form, 0 for the general 7-array form; kernels launched. */
+int eaf_cg_last_timing(eaf_cg_t h, double* solve_ms, double* kernel_ms,
+                       int* symmetric, int* kernels);
+
+/* Device time of the last host-pointer solve from the first upload to the
+ * end of the phi download, in milliseconds. */
+double eaf_cg_last_e2e_ms(eaf_cg_t h);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their
+ * own device work against the solver. */
+void* eaf_cg_stream(eaf_cg_t h);
+
+/* Pinned host memory helpers (cudaHostAlloc / cudaFreeHost). */
+int eaf_host_alloc(void** ptr, size_t bytes);
+int eaf_host_free(void* ptr);
+/* Page-lock an existing host range for faster uploads (cudaHostRegister). */
+int eaf_host_register(void* ptr, size_t bytes);
+int eaf_host_unregister(void* ptr);
+
+/* Self-test of the bounded barrier: launches two blocks that wait at a group
+ * barrier whose arrival target can never be met, with the given bound. It
+ * must return EAF_ETIMEOUT after about timeout_ms, with the device context
+ * intact. No reference counterpart (failure-detection test hook). */
+int eaf_selftest_barrier_timeout(int device, double timeout_ms);
+
+/* Library version string. */
+const char* eaf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EAFCG_H */

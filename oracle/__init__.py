@@ -1,0 +1,104 @@
+"""ctypes loader for the oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle is a CPU restatement of the reference CG ``cg_3d_mpi``
+(src/mod_solver_3d.f90:485-620); see eaf_oracle.c for the line-by-line
+mapping. Only tests, the smoke check and the CPU-baseline legs of bench.py
+use it, always as the checker or the timed CPU reference, never as the
+product path. Parity is unpinned at the CG boundary: no reference binary or
+reference CG golden vector exists to pin it against.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libeaforacle.so")
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        ci, cd = ctypes.c_int, ctypes.c_double
+        L.eaf_oracle_cg.argtypes = [ci, ci, ci] + [_dp] * 9 + [ci, cd, _dp,
+                                                               ctypes.POINTER(ci)]
+        L.eaf_oracle_cg.restype = ci
+        L.eaf_oracle_cg_threads.argtypes = (L.eaf_oracle_cg.argtypes + [ci])
+        L.eaf_oracle_cg_threads.restype = ci
+        L.eaf_oracle_cg_tree.argtypes = (L.eaf_oracle_cg.argtypes + [ci, ci])
+        L.eaf_oracle_cg_tree.restype = ci
+        L.eaf_oracle_dot.argtypes = [ci, ci, ci, _dp, _dp, ci, ci]
+        L.eaf_oracle_dot.restype = cd
+        L.eaf_oracle_matvec.argtypes = [ci, ci, ci] + [_dp] * 9
+        L.eaf_oracle_matvec.restype = None
+        L.eaf_oracle_theta_wrap.argtypes = [ci, ci, ci, _dp]
+        L.eaf_oracle_theta_wrap.restype = None
+        L.eaf_oracle_max_threads.argtypes = []
+        L.eaf_oracle_max_threads.restype = ci
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def cg(system, phi: np.ndarray, max_iter: int, tol: float, nthreads: int = 1,
+       plan: tuple | None = None):
+    """Solve in place on ``phi`` (halo layout). Returns (residual, n_iter).
+
+    ``plan=(G, B)`` associates the dot products as the CUDA kernels do for a
+    launch of G blocks x B threads (everything else is unchanged); the default
+    is the reference's sequential sum.
+    """
+    res = ctypes.c_double(0.0)
+    nit = ctypes.c_int(0)
+    args = [system.nr, system.nth, system.nz] + [_p(a) for a in system.arrays()]
+    args += [_p(phi), int(max_iter), float(tol), ctypes.byref(res),
+             ctypes.byref(nit)]
+    if plan is not None:
+        rc = lib().eaf_oracle_cg_tree(*args, int(plan[0]), int(plan[1]))
+    elif nthreads == 1:
+        rc = lib().eaf_oracle_cg(*args)
+    else:
+        rc = lib().eaf_oracle_cg_threads(*args, int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle cg failed with status {rc}")
+    return res.value, nit.value
+
+
+def matvec(system, x: np.ndarray) -> np.ndarray:
+    """Reference matvec: refreshes x's theta halos in place, returns y."""
+    y = np.zeros_like(x)
+    args = [system.nr, system.nth, system.nz] + [_p(a) for a in system.arrays()[:7]]
+    lib().eaf_oracle_matvec(*args, _p(x), _p(y))
+    return y
+
+
+def dot(nr: int, nth: int, nz: int, a: np.ndarray, b: np.ndarray,
+        plan: tuple | None = None) -> float:
+    G, B = plan if plan is not None else (0, 0)
+    return lib().eaf_oracle_dot(nr, nth, nz, _p(a), _p(b), int(G), int(B))
+
+
+def theta_wrap(nr: int, nth: int, nz: int, x: np.ndarray) -> None:
+    lib().eaf_oracle_theta_wrap(nr, nth, nz, _p(x))
+
+
+def max_threads() -> int:
+    return lib().eaf_oracle_max_threads()
