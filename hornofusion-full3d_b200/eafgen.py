@@ -193,7 +193,8 @@ def draw_rhs(rng: np.random.Generator, nr: int, nth: int, nz: int) -> np.ndarray
     b = rng.normal(0.0, 1e-3, size=(nz, nth, nr))
     free = np.ones_like(b, dtype=bool)
     free[0, 0, nr - 1] = False
-    b[free] -= b[free].mean()
+    if free.any():
+        b[free] -= b[free].mean()
     b[0, 0, nr - 1] = 0.0
     return b
 
