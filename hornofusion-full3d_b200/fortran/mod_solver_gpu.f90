@@ -1,0 +1,148 @@
+!===============================================================================
+! mod_solver_gpu.f90 - iso_c_binding interface to libeafcg.so (the B200
+! pressure-correction CG) and a drop-in replacement for cg_3d_mpi.
+!
+! The reference call in solve_pressure_correction
+! (src/mod_pressure_3d.f90:316-318)
+!     call cg_3d_mpi(aW, aE, aS, aN, aB, aT, aP, Su, sh%pp, m, &
+!                    cfg%max_inner_pres, SOR_TOL_PRESSURE, cg_res, n_iter_cg)
+! becomes
+!     call cg_3d_gpu(aW, aE, aS, aN, aB, aT, aP, Su, sh%pp, m, &
+!                    cfg%max_inner_pres, SOR_TOL_PRESSURE, cg_res, n_iter_cg)
+! with the same dummies and meaning as cg_3d_mpi (src/mod_solver_3d.f90:
+! 485-496). The workspace arrays are contiguous allocatables
+! (src/mod_workspace.f90:120-126), so they pass to the C entry point without
+! copies. Not compiled in this repository's build (no Fortran compiler is
+! available where it is built); link with -L<dir> -leafcg.
+!===============================================================================
+module mod_solver_gpu
+    use iso_c_binding
+    implicit none
+    private
+    public :: cg_3d_gpu, cg_3d_gpu_mixed, cg_gpu_release
+    public :: eaf_cg_create, eaf_cg_destroy, eaf_cg_solve_f64, eaf_cg_solve_mixed
+
+    integer(c_int), parameter, public :: EAF_OK = 0, EAF_ENONFINITE = 3
+
+    interface
+        integer(c_int) function eaf_cg_create(h, nr, nth, nz, device) &
+                bind(C, name="eaf_cg_create")
+            import :: c_int, c_ptr
+            type(c_ptr), intent(out) :: h
+            integer(c_int), value :: nr, nth, nz, device
+        end function eaf_cg_create
+
+        integer(c_int) function eaf_cg_destroy(h) bind(C, name="eaf_cg_destroy")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function eaf_cg_destroy
+
+        integer(c_int) function eaf_cg_solve_f64(h, aW, aE, aS, aN, aB, aT, aP, &
+                Su, phi, max_iter, tol, residual, n_iter) &
+                bind(C, name="eaf_cg_solve_f64")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: aW(*), aE(*), aS(*), aN(*)
+            real(c_double), intent(in) :: aB(*), aT(*), aP(*), Su(*)
+            real(c_double), intent(inout) :: phi(*)
+            integer(c_int), value :: max_iter
+            real(c_double), value :: tol
+            real(c_double), intent(out) :: residual
+            integer(c_int), intent(out) :: n_iter
+        end function eaf_cg_solve_f64
+
+        integer(c_int) function eaf_cg_solve_mixed(h, aW, aE, aS, aN, aB, aT, &
+                aP, Su, phi, max_outer, max_inner, tol, inner_tol, residual, &
+                n_iter, n_outer) bind(C, name="eaf_cg_solve_mixed")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: aW(*), aE(*), aS(*), aN(*)
+            real(c_double), intent(in) :: aB(*), aT(*), aP(*), Su(*)
+            real(c_double), intent(inout) :: phi(*)
+            integer(c_int), value :: max_outer, max_inner
+            real(c_double), value :: tol, inner_tol
+            real(c_double), intent(out) :: residual
+            integer(c_int), intent(out) :: n_iter, n_outer
+        end function eaf_cg_solve_mixed
+    end interface
+
+    ! One handle per mesh size, kept across SIMPLE iterations like the
+    ! reference's persistent workspace (src/mod_workspace.f90:120-144).
+    type(c_ptr), save :: handle = c_null_ptr
+    integer, save :: h_nr = -1, h_nth = -1, h_nz = -1
+
+contains
+
+    subroutine ensure_handle(nr, nth, nz)
+        integer, intent(in) :: nr, nth, nz
+        integer(c_int) :: st
+        if (c_associated(handle) .and. nr == h_nr .and. nth == h_nth &
+            .and. nz == h_nz) return
+        if (c_associated(handle)) st = eaf_cg_destroy(handle)
+        st = eaf_cg_create(handle, int(nr, c_int), int(nth, c_int), &
+                           int(nz, c_int), 0_c_int)
+        if (st /= EAF_OK) error stop 'eaf_cg_create failed'
+        h_nr = nr; h_nth = nth; h_nz = nz
+    end subroutine ensure_handle
+
+    ! Same dummies as cg_3d_mpi; serial meshes only (the whole theta x z
+    ! domain on one GPU). A NaN residual is returned like the reference's.
+    subroutine cg_3d_gpu(aW, aE, aS, aN, aB, aT, aP, Su, phi, m, &
+                         max_iter, tol, residual, n_iter)
+        use mod_constants, only: dp
+        use mod_types_3d, only: mesh_t
+        real(dp), intent(in), contiguous  :: aW(-1:,-1:,-1:), aE(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aS(-1:,-1:,-1:), aN(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aB(-1:,-1:,-1:), aT(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aP(-1:,-1:,-1:), Su(-1:,-1:,-1:)
+        real(dp), intent(inout), contiguous :: phi(-1:,-1:,-1:)
+        type(mesh_t), intent(in) :: m
+        integer, intent(in)      :: max_iter
+        real(dp), intent(in)     :: tol
+        real(dp), intent(out)    :: residual
+        integer, intent(out)     :: n_iter
+        integer(c_int) :: st, nit
+        real(c_double) :: res
+        if (m%is_parallel) error stop 'cg_3d_gpu: decomposed meshes are not supported'
+        call ensure_handle(m%nr, m%ntheta, m%nz)
+        st = eaf_cg_solve_f64(handle, aW, aE, aS, aN, aB, aT, aP, Su, phi, &
+                              int(max_iter, c_int), real(tol, c_double), res, nit)
+        if (st /= EAF_OK .and. st /= EAF_ENONFINITE) error stop 'eaf_cg_solve_f64 failed'
+        residual = res
+        n_iter = nit
+    end subroutine cg_3d_gpu
+
+    ! Mixed FP32/FP64 form (no reference counterpart): same arrays.
+    subroutine cg_3d_gpu_mixed(aW, aE, aS, aN, aB, aT, aP, Su, phi, m, &
+                               tol, residual, n_iter)
+        use mod_constants, only: dp
+        use mod_types_3d, only: mesh_t
+        real(dp), intent(in), contiguous  :: aW(-1:,-1:,-1:), aE(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aS(-1:,-1:,-1:), aN(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aB(-1:,-1:,-1:), aT(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aP(-1:,-1:,-1:), Su(-1:,-1:,-1:)
+        real(dp), intent(inout), contiguous :: phi(-1:,-1:,-1:)
+        type(mesh_t), intent(in) :: m
+        real(dp), intent(in)     :: tol
+        real(dp), intent(out)    :: residual
+        integer, intent(out)     :: n_iter
+        integer(c_int) :: st, nit, nout
+        real(c_double) :: res
+        if (m%is_parallel) error stop 'cg_3d_gpu_mixed: decomposed meshes are not supported'
+        call ensure_handle(m%nr, m%ntheta, m%nz)
+        st = eaf_cg_solve_mixed(handle, aW, aE, aS, aN, aB, aT, aP, Su, phi, &
+                                200_c_int, 100000_c_int, real(tol, c_double), &
+                                0.1_c_double, res, nit, nout)
+        if (st /= EAF_OK .and. st /= EAF_ENONFINITE) error stop 'eaf_cg_solve_mixed failed'
+        residual = res
+        n_iter = nit
+    end subroutine cg_3d_gpu_mixed
+
+    subroutine cg_gpu_release()
+        integer(c_int) :: st
+        if (c_associated(handle)) st = eaf_cg_destroy(handle)
+        handle = c_null_ptr
+        h_nr = -1; h_nth = -1; h_nz = -1
+    end subroutine cg_gpu_release
+
+end module mod_solver_gpu
