@@ -21,6 +21,7 @@ EAF_ENOMEM = 6
 EAF_EADMIT = 7
 EAF_EBUSY = 8
 EAF_ECLOSED = 9
+EAF_NOALLOC_MAX_CELLS = 32768
 
 STATUS_NAMES = {
     0: "EAF_OK", 1: "EAF_ECUDA", 2: "EAF_EINVAL", 3: "EAF_ENONFINITE",
@@ -58,6 +59,8 @@ SIGNATURES = [
     ("eaf_host_register", _ci, [_vp, _sz]),
     ("eaf_host_unregister", _ci, [_vp]),
     ("eaf_selftest_barrier_timeout", _ci, [_ci, _cd]),
+    ("eaf_cg_solve_f64_noalloc", _ci,
+     [_ci, _ci, _ci, _ci, _vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
 ]
 
 _lib = None

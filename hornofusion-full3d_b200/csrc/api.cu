@@ -55,6 +55,10 @@ void set_error(const char* what, cudaError_t e) {
            e == cudaSuccess ? "ok" : cudaGetErrorString(e));
 }
 
+void set_error_text(const char* msg) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+}
+
 DeviceGuard::DeviceGuard(int dev) : prev_(-1), ok_(false) {
   if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
   ok_ = cudaSetDevice(dev) == cudaSuccess;

@@ -7,6 +7,8 @@ namespace eaf {
 
 // Records the last CUDA failure of this thread for eaf_last_error().
 void set_error(const char* what, cudaError_t e);
+// Records a plain message (no CUDA error) for eaf_last_error().
+void set_error_text(const char* msg);
 
 // Makes `dev` current for the lifetime of the guard and restores the
 // caller's device afterwards.

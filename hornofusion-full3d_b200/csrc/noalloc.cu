@@ -1,0 +1,177 @@
+// eaf_cg_solve_f64_noalloc: the plain FP64 solve for callers that must not
+// allocate device memory.
+//
+// Who cannot allocate, and why: a simulator whose device memory is owned end
+// to end by its own pool allocator or fixed budget (a cudaMalloc behind its
+// back either fails or fragments that pool), and code on a latency-critical
+// path, where cudaMalloc/cudaFree would synchronise the device and stall
+// every other stream. Such a caller owns its inputs and phi and hands them
+// over; everything else this solve needs lives in one file-scope device
+// array that each GPU holds from library load until process exit.
+//
+// Limits and sharing rules:
+//   * at most kNoallocMaxCells = EAF_NOALLOC_MAX_CELLS interior cells
+//     (32768; 18x36x24 fits, 35x70x50 does not); larger meshes are refused
+//     with EAF_EINVAL and an explanatory eaf_last_error() text;
+//   * the array is shared by every call on a device and keeps the previous
+//     call's contents; each call re-packs the inputs and zeroes the barrier
+//     counter, the error word and the symmetry flag before its solver runs;
+//   * two calls whose work overlaps on the same GPU (different host threads,
+//     or different streams not ordered by the caller) race on the array.
+//     Callers serialise their calls per device;
+//   * the first call on a device looks the array's device address up with
+//     cudaGetSymbolAddress (once per device, with that device current). That
+//     first call should therefore come before any stream capture begins on
+//     the device.
+// The kernels are the ones eaf_cg_solve_f64_device runs (pack, persistent
+// cooperative CG, unpack), launched with the same default shape, so results
+// are bit-identical to that entry point on the same inputs.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <mutex>
+
+#include "cg_kernels.h"
+#include "eafcg.h"
+#include "eafcg_internal.h"
+
+namespace {
+
+constexpr int kNoallocMaxCells = EAF_NOALLOC_MAX_CELLS;
+constexpr int kNoallocMaxBlocks = 64;
+constexpr int kPartSlots = 8;
+constexpr int kMaxDevices = 64;
+constexpr uint64_t kNoallocTimeoutNs = 2000ull * 1000ull * 1000ull;
+
+// Scratch layout (doubles unless stated):
+//   12 compact arrays of kNoallocMaxCells: aP aE aN aT aW aS aB b x r p q
+//   partial table: kPartSlots * kNoallocMaxBlocks
+//   barrier counter (u64), error word (int), symmetry flag (int), result
+constexpr size_t kArrays = 12;
+constexpr size_t kPartOff = kArrays * kNoallocMaxCells;
+constexpr size_t kCounterOff = kPartOff + (size_t)kPartSlots * kNoallocMaxBlocks;
+constexpr size_t kErrOff = kCounterOff + 1;    // one double slot each
+constexpr size_t kAsymOff = kErrOff + 1;
+constexpr size_t kResultOff = kAsymOff + 1;
+constexpr size_t kScratchDoubles =
+    kResultOff + (sizeof(eaf::SolveResult) + sizeof(double) - 1) / sizeof(double);
+
+static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+
+struct DeviceSlot {
+  std::once_flag once;
+  cudaError_t status = cudaSuccess;
+  double* base = nullptr;
+};
+DeviceSlot g_slots[kMaxDevices];
+
+// Device address of the scratch array on the current device `dev`.
+cudaError_t scratch_on(int dev, double** out) {
+  DeviceSlot& s = g_slots[dev];
+  std::call_once(s.once, [&s]() {
+    void* p = nullptr;
+    s.status = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    s.base = static_cast<double*>(p);
+  });
+  *out = s.base;
+  return s.status;
+}
+
+int max_coresident(int block, int dev) {
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eaf::cg_f64_kernel_ptr(),
+                                                    block, 0) != cudaSuccess)
+    return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 0;
+  return per_sm * sms;
+}
+
+}  // namespace
+
+extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
+                                        void* stream, const double* aW,
+                                        const double* aE, const double* aS,
+                                        const double* aN, const double* aB,
+                                        const double* aT, const double* aP,
+                                        const double* Su, double* phi, int max_iter,
+                                        double tol, double* residual, int* n_iter) {
+  if (!aW || !aE || !aS || !aN || !aB || !aT || !aP || !Su || !phi || !residual ||
+      !n_iter || nr < 1 || nth < 1 || nz < 1 || device < 0 || device >= kMaxDevices)
+    return EAF_EINVAL;
+  const long long n = (long long)nr * nth * nz;
+  if (n > kNoallocMaxCells) {
+    char msg[160];
+    snprintf(msg, sizeof(msg),
+             "eaf_cg_solve_f64_noalloc: %lld cells exceed the %d-cell static "
+             "scratch; use eaf_cg_create/eaf_cg_solve_f64_device",
+             n, kNoallocMaxCells);
+    eaf::set_error_text(msg);
+    return EAF_EINVAL;
+  }
+  eaf::DeviceGuard guard(device);
+  if (!guard.ok()) {
+    eaf::set_error("eaf_cg_solve_f64_noalloc: cudaSetDevice", cudaErrorInvalidDevice);
+    return EAF_ECUDA;
+  }
+  double* base = nullptr;
+  cudaError_t e = scratch_on(device, &base);
+  if (e != cudaSuccess || !base) {
+    eaf::set_error("eaf_cg_solve_f64_noalloc: cudaGetSymbolAddress", e);
+    return EAF_ECUDA;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const eaf::MeshDims d = eaf::make_dims(nr, nth, nz);
+  const size_t M = kNoallocMaxCells;
+  eaf::SysF64 s;
+  s.aP = base + 0 * M;
+  s.aE = base + 1 * M;
+  s.aN = base + 2 * M;
+  s.aT = base + 3 * M;
+  s.aW = base + 4 * M;
+  s.aS = base + 5 * M;
+  s.aB = base + 6 * M;
+  s.b = base + 7 * M;
+  s.x = base + 8 * M;
+  s.r = base + 9 * M;
+  s.p = base + 10 * M;
+  s.q = base + 11 * M;
+  s.asym = reinterpret_cast<int*>(base + kAsymOff);
+  eaf::GroupWs ws;
+  ws.part = base + kPartOff;
+  ws.counter = reinterpret_cast<unsigned long long*>(base + kCounterOff);
+  ws.err = reinterpret_cast<int*>(base + kErrOff);
+  ws.result = reinterpret_cast<eaf::SolveResult*>(base + kResultOff);
+
+  // Launch shape: the default of eaf_cg_create handles (one 1024-thread
+  // block up to 8192 cells, else one 512-thread block per 2048 cells),
+  // capped by co-residency and by the partial table's kNoallocMaxBlocks.
+  int block = 512, grid;
+  if (n <= 8192) {
+    block = 1024;
+    grid = 1;
+  } else {
+    grid = (int)((n + 2047) / 2048);
+  }
+  const int cap = max_coresident(block, device);
+  if (cap > 0 && grid > cap) grid = cap;
+  if (grid > kNoallocMaxBlocks) grid = kNoallocMaxBlocks;
+
+  eaf::HaloInputs in = {aW, aE, aS, aN, aB, aT, aP, Su, phi};
+  e = eaf::launch_pack_f64(d, in, s, st);
+  if (e == cudaSuccess)
+    e = eaf::launch_cg_f64(d, s, ws, max_iter, tol, kNoallocTimeoutNs, grid, block, st);
+  if (e == cudaSuccess) e = eaf::launch_unpack_f64(d, s.x, phi, st);
+  eaf::SolveResult r;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&r, ws.result, sizeof(r), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    eaf::set_error("eaf_cg_solve_f64_noalloc", e);
+    return EAF_ECUDA;
+  }
+  *residual = r.residual;
+  *n_iter = r.n_iter;
+  return r.status;
+}

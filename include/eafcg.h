@@ -148,6 +148,30 @@ int eaf_host_free(void* ptr);
 int eaf_host_register(void* ptr, size_t bytes);
 int eaf_host_unregister(void* ptr);
 
+/* ---- no-allocation entry point ----------------------------------------- */
+/* No counterpart in the reference. For callers that must not allocate
+ * device memory: a simulator whose device memory is owned by its own pool
+ * allocator or fixed budget, or code on a latency-critical path where
+ * cudaMalloc/cudaFree would synchronise the device. Same contract and
+ * result as eaf_cg_solve_f64_device (device pointers, reference layout),
+ * but without a handle: all working memory is one static device array of
+ * EAF_NOALLOC_MAX_CELLS cells' worth (about 3 MiB) that every GPU loading
+ * the library holds until process exit. Larger meshes return EAF_EINVAL
+ * (see eaf_last_error()). The array is shared by all calls on a device and
+ * keeps the last call's contents; calls whose GPU work overlaps on one
+ * device race, so serialise them. The first call on a device looks up the
+ * array's device address and should come before any stream capture on
+ * that device. `stream` is a cudaStream_t (NULL: the default stream); the
+ * call returns after the stream has finished the solve. */
+#define EAF_NOALLOC_MAX_CELLS 32768
+int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device, void* stream,
+                             const double* aW, const double* aE,
+                             const double* aS, const double* aN,
+                             const double* aB, const double* aT,
+                             const double* aP, const double* Su, double* phi,
+                             int max_iter, double tol, double* residual,
+                             int* n_iter);
+
 /* Self-test of the bounded barrier: launches two blocks that wait at a group
  * barrier whose arrival target can never be met, with the given bound. It
  * must return EAF_ETIMEOUT after about timeout_ms, with the device context
