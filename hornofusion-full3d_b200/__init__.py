@@ -132,6 +132,12 @@ class CGSolver:
         check(self._lib.eaf_cg_get_launch(self._h, ctypes.byref(b), ctypes.byref(g)))
         return b.value, g.value
 
+    def last_launch(self) -> tuple:
+        """(grid, block) of the last solve: the oracle plan of its dots."""
+        b, g = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.eaf_cg_last_launch(self._h, ctypes.byref(b), ctypes.byref(g)))
+        return g.value, b.value
+
     def set_timeout_ms(self, ms: float) -> None:
         check(self._lib.eaf_cg_set_timeout_ms(self._h, float(ms)), "set_timeout")
 

@@ -51,6 +51,7 @@ SIGNATURES = [
     ("eaf_cg_set_launch", _ci, [_vp, _ci, _ci]),
     ("eaf_cg_get_launch", _ci, [_vp, _pi, _pi]),
     ("eaf_cg_set_timeout_ms", _ci, [_vp, _cd]),
+    ("eaf_cg_last_launch", _ci, [_vp, _pi, _pi]),
     ("eaf_cg_last_timing", _ci, [_vp, _pd, _pd, _pi, _pi]),
     ("eaf_cg_last_e2e_ms", _cd, [_vp]),
     ("eaf_cg_stream", _vp, [_vp]),
@@ -59,6 +60,7 @@ SIGNATURES = [
     ("eaf_host_register", _ci, [_vp, _sz]),
     ("eaf_host_unregister", _ci, [_vp]),
     ("eaf_selftest_barrier_timeout", _ci, [_ci, _cd]),
+    ("eaf_diag_allreduce_us", _ci, [_ci, _ci, _ci, _ci, _ci, _pd]),
     ("eaf_cg_solve_f64_noalloc", _ci,
      [_ci, _ci, _ci, _ci, _vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
 ]

@@ -35,6 +35,7 @@ UNITS = {
     "cg_batch.cu": [],
     "noalloc.cu": ["-fmad=false"],
     "serve.cu": [],
+    "diag.cu": [],
 }
 
 

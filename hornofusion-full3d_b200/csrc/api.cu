@@ -44,6 +44,7 @@ struct eaf_cg {
   cudaEvent_t ev[6];   // e2e0, solve0, kern0, kern1, solve1, e2e1
   double last_solve_ms, last_kernel_ms, last_e2e_ms;
   int last_sym, last_kernels;
+  int last_grid, last_block;
 };
 
 namespace eaf {
@@ -82,8 +83,8 @@ using eaf::set_error;
 
 static void free_handle(eaf_cg* h) {
   for (int i = 0; i < 9; ++i) cudaFree(h->stage[i]);
-  double* f64[] = {h->s.aP, h->s.aE, h->s.aN, h->s.aT, h->s.aW, h->s.aS,
-                   h->s.aB, h->s.b,  h->s.x,  h->s.r,  h->s.p,  h->s.q};
+  double* f64[] = {h->s.aP, h->s.aE, h->s.aN, h->s.aT, h->s.aW, h->s.aS, h->s.aB,
+                   h->s.b,  h->s.x,  h->s.r,  h->s.p,  h->s.q,  h->s.p2, h->s.z};
   for (double* p : f64) cudaFree(p);
   cudaFree(h->s.asym);
   float* f32[] = {h->f.aP, h->f.aE, h->f.aN, h->f.aT, h->f.aW, h->f.aS, h->f.aB,
@@ -181,14 +182,16 @@ int eaf_cg_create_mesh(eaf_cg_t* out, int nr, int nth, int nz, int is_parallel,
   };
   e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
   for (int i = 0; i < 9; ++i) alloc((void**)&h->stage[i], h->nh * sizeof(double));
-  double** f64[] = {&h->s.aP, &h->s.aE, &h->s.aN, &h->s.aT, &h->s.aW, &h->s.aS,
-                    &h->s.aB, &h->s.b,  &h->s.x,  &h->s.r,  &h->s.p,  &h->s.q};
+  double** f64[] = {&h->s.aP, &h->s.aE, &h->s.aN, &h->s.aT, &h->s.aW,
+                    &h->s.aS, &h->s.aB, &h->s.b,  &h->s.x,  &h->s.r,
+                    &h->s.p,  &h->s.q,  &h->s.p2, &h->s.z};
   for (double** p : f64) alloc((void**)p, (size_t)n * sizeof(double));
   alloc((void**)&h->s.asym, sizeof(int));
   int dev_sms = 0;
   if (e == cudaSuccess)
     e = cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
   h->sms = dev_sms > 0 ? dev_sms : 148;
+
   alloc((void**)&h->ws.part, sizeof(double) * kPartSlots * h->sms * 8);
   alloc((void**)&h->ws.counter, sizeof(unsigned long long));
   alloc((void**)&h->ws.err, sizeof(int));
@@ -233,6 +236,13 @@ int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks) {
   if (!h || !block_threads || !grid_blocks) return EAF_EINVAL;
   eaf::DeviceGuard guard(h->device);
   pick_launch(h, eaf::cg_f64_kernel_ptr(), grid_blocks, block_threads);
+  return EAF_OK;
+}
+
+int eaf_cg_last_launch(eaf_cg_t h, int* block_threads, int* grid_blocks) {
+  if (!h || !block_threads || !grid_blocks) return EAF_EINVAL;
+  *block_threads = h->last_block;
+  *grid_blocks = h->last_grid;
   return EAF_OK;
 }
 
@@ -336,6 +346,8 @@ int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts&
     EAF_CUDA(eaf::launch_cg_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
                                 grid, block, h->st));
   }
+  h->last_grid = grid;
+  h->last_block = block;
   EAF_CUDA(cudaEventRecord(h->ev[3], h->st));
   EAF_CUDA(eaf::launch_unpack_f64(h->d, h->s.x, phi, h->st));
   EAF_CUDA(cudaEventRecord(h->ev[4], h->st));
@@ -480,6 +492,7 @@ __global__ void barrier_selftest_kernel(GroupWs ws, uint64_t timeout_ns) {
   g.counter = ws.counter;
   g.err = ws.err;
   g.part = ws.part;
+  g.stage = group_stage_smem();
   g.nb = 3;
   g.bid = blockIdx.x;
   g.timeout_ns = timeout_ns;

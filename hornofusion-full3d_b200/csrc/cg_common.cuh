@@ -27,7 +27,7 @@ constexpr double kSmall = 1.0e-30;  // SMALL, src/mod_constants.f90:53
 struct FastDiv {
   uint32_t d, m, s;
   __host__ __device__ FastDiv() : d(1), m(1), s(0) {}
-  __host__ explicit FastDiv(uint32_t div) : d(div) {
+  __host__ __device__ explicit FastDiv(uint32_t div) : d(div) {
     s = 0;
     while ((1ull << s) < d) ++s;
     m = (uint32_t)(((1ull << 32) * ((1ull << s) - d)) / d + 1);
@@ -81,16 +81,41 @@ __device__ __forceinline__ uint64_t global_ns() {
 // on expiry the waiter records EAF_ETIMEOUT in the shared error word and all
 // waiters of the group leave. A group of one block only needs __syncthreads.
 // ---------------------------------------------------------------------------
+// Largest group of a persistent launch (blocks) and most sums reduced at
+// once; the launchers never exceed them.
+constexpr int kMaxGroupBlocks = 1184;
+constexpr int kMaxGroupSlots = 3;
+
 struct Group {
   unsigned long long* counter;
   int* err;
   double* part;       // [slots][nb] block partials of this group
+  double* stage;      // shared memory for kMaxGroupSlots * nb partials
   int nb;             // blocks in the group
   int bid;            // this block's index in the group
   uint64_t timeout_ns;
   unsigned long long epoch;  // barriers passed (meaningful in thread 0)
 };
 
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
+// Memory-ordering forms of the group barrier (all correct under the PTX
+// memory model; they differ in cost):
+//   0  full fences around a release add, acquire polls;
+//   1  release add after the CTA barrier, acquire polls, no extra fences
+//      (bar.sync orders the block's writes before thread 0's release, and
+//      the acquire that observes the last arrival orders what follows);
+//   2  release add, relaxed polls, one acquire fence after the last poll.
+constexpr int kBarrierForm = 1;
+
+template <int FORM = kBarrierForm>
 __device__ __forceinline__ bool group_barrier(Group& g) {
   __shared__ int s_ok;
   if (g.nb == 1) {
@@ -101,20 +126,24 @@ __device__ __forceinline__ bool group_barrier(Group& g) {
   if (threadIdx.x == 0) {
     g.epoch += 1;
     const unsigned long long target = g.epoch * (unsigned long long)g.nb;
-    __threadfence();
+    if (FORM == 0) __threadfence();
     red_release_add_u64(g.counter, 1ull);
     int ok = 1;
-    const uint64_t t0 = global_ns();
+    uint64_t t0 = 0;
     uint32_t spins = 0;
-    while (ld_acquire_u64(g.counter) < target) {
-      if (ld_volatile_i32(g.err) != 0) { ok = 0; break; }
-      if ((++spins & 63u) == 0 && global_ns() - t0 > g.timeout_ns) {
-        atomicCAS(g.err, 0, (int)EAF_ETIMEOUT);
-        ok = 0;
-        break;
+    while ((FORM == 2 ? ld_relaxed_u64(g.counter) : ld_acquire_u64(g.counter)) < target) {
+      if ((++spins & 63u) == 0) {
+        if (spins == 64u) t0 = global_ns();
+        if (ld_volatile_i32(g.err) != 0) { ok = 0; break; }
+        if (global_ns() - t0 > g.timeout_ns) {
+          atomicCAS(g.err, 0, (int)EAF_ETIMEOUT);
+          ok = 0;
+          break;
+        }
       }
     }
-    __threadfence();
+    if (FORM == 0) __threadfence();
+    if (FORM == 2) fence_acq_rel_gpu();
     s_ok = ok;
   }
   __syncthreads();
@@ -156,11 +185,19 @@ __device__ __forceinline__ void block_sum_to_thread0(T (&v)[NV]) {
   }
 }
 
+// Static shared staging buffer for kernels whose groups may hold up to
+// kMaxGroupBlocks blocks (a single definition, so all uses in a kernel
+// share it). Kernels with dynamic shared memory carve their own instead.
+static __device__ __forceinline__ double* group_stage_smem() {
+  __shared__ double s_stage[kMaxGroupSlots * kMaxGroupBlocks];
+  return s_stage;
+}
+
 // Group all-reduce of NV sums. Per-thread and in-block sums are carried in
 // T (FP32 for the mixed-precision inner solve, FP64 otherwise); block
 // partials go to slots [slot, slot+NV) of the group's FP64 partial table and
 // are folded in FP64. Returns false if the barrier gave up.
-template <int NV, typename T>
+template <int NV, typename T, int FORM = kBarrierForm>
 __device__ __forceinline__ bool group_allsum(T (&v)[NV], Group& g, int slot) {
   __shared__ double s_tot[NV];
   block_sum_to_thread0<NV, T>(v);
@@ -179,14 +216,35 @@ __device__ __forceinline__ bool group_allsum(T (&v)[NV], Group& g, int slot) {
 #pragma unroll
     for (int m = 0; m < NV; ++m) g.part[(size_t)(slot + m) * g.nb + g.bid] = (double)v[m];
   }
-  const bool ok = group_barrier(g);
+  const bool ok = group_barrier<FORM>(g);
+  // Stage the NV x nb partials in shared memory with independent loads (all
+  // in flight at once), then fold them in the fixed order: lane l of warp 0
+  // sums partials l, l+32, ... sequentially, and the lanes are folded by the
+  // butterfly.
+  double* s_part = g.stage;
+  const int total = NV * g.nb;
+  const double* src = g.part + (size_t)slot * g.nb;
+  for (int i0 = threadIdx.x; i0 < total; i0 += 4 * (int)blockDim.x) {
+    double t[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * (int)blockDim.x;
+      t[u] = i < total ? __ldcg(src + i) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * (int)blockDim.x;
+      if (i < total) s_part[i] = t[u];
+    }
+  }
+  __syncthreads();
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
 #pragma unroll
     for (int m = 0; m < NV; ++m) {
-      const double* p = g.part + (size_t)(slot + m) * g.nb;
+      const double* p = s_part + m * g.nb;
       double s = 0.0;
-      for (int b = lane; b < g.nb; b += 32) s = s + __ldcg(p + b);
+      for (int b = lane; b < g.nb; b += 32) s = s + p[b];
       s = warp_allsum(s);
       if (lane == 0) s_tot[m] = s;
     }
@@ -194,6 +252,94 @@ __device__ __forceinline__ bool group_allsum(T (&v)[NV], Group& g, int slot) {
   __syncthreads();
 #pragma unroll
   for (int m = 0; m < NV; ++m) v[m] = (T)s_tot[m];
+  return ok;
+}
+
+// Split-phase form of group_allsum: group_arrive publishes this block's
+// partials and its arrival (thread 0, after the block fold); the caller may
+// then do work that neither reads the totals nor touches the reduction's
+// shared buffers, and group_wait completes the reduction. Same association
+// as group_allsum.
+template <int NV, typename T>
+__device__ __forceinline__ void group_arrive(T (&v)[NV], Group& g, int slot) {
+  __shared__ double s_blk[NV];
+  block_sum_to_thread0<NV, T>(v);
+  if (threadIdx.x == 0) {
+    if (g.nb == 1) {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) s_blk[m] = (double)v[m];
+    } else {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) g.part[(size_t)(slot + m) * g.nb + g.bid] = (double)v[m];
+      g.epoch += 1;
+      red_release_add_u64(g.counter, 1ull);
+    }
+  }
+  if (g.nb == 1) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < NV; ++m) v[m] = (T)s_blk[m];
+    __syncthreads();
+  }
+}
+
+template <int NV, typename T>
+__device__ __forceinline__ bool group_wait(T (&v)[NV], Group& g, int slot) {
+  if (g.nb == 1) return true;  // completed in group_arrive
+  __shared__ int s_ok;
+  __shared__ double s_tot[NV];
+  if (threadIdx.x == 0) {
+    const unsigned long long target = g.epoch * (unsigned long long)g.nb;
+    int ok = 1;
+    uint64_t t0 = 0;
+    uint32_t spins = 0;
+    while (ld_acquire_u64(g.counter) < target) {
+      if ((++spins & 63u) == 0) {
+        if (spins == 64u) t0 = global_ns();
+        if (ld_volatile_i32(g.err) != 0) { ok = 0; break; }
+        if (global_ns() - t0 > g.timeout_ns) {
+          atomicCAS(g.err, 0, (int)EAF_ETIMEOUT);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  double* s_part = g.stage;
+  const int total = NV * g.nb;
+  const double* src = g.part + (size_t)slot * g.nb;
+  for (int i0 = threadIdx.x; i0 < total; i0 += 4 * (int)blockDim.x) {
+    double t[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * (int)blockDim.x;
+      t[u] = i < total ? __ldcg(src + i) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * (int)blockDim.x;
+      if (i < total) s_part[i] = t[u];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      const double* p = s_part + m * g.nb;
+      double s = 0.0;
+      for (int b = lane; b < g.nb; b += 32) s = s + p[b];
+      s = warp_allsum(s);
+      if (lane == 0) s_tot[m] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < NV; ++m) v[m] = (T)s_tot[m];
+  const bool ok = s_ok != 0;
+  __syncthreads();
   return ok;
 }
 

@@ -8,11 +8,12 @@
 //
 // One persistent cooperative launch runs the whole solve. Each block owns a
 // contiguous slice of cells (compact layout, cg_common.cuh) in every phase;
-// an iteration is three phases separated by group barriers:
-//   S0  q = A p, partial p.q                       -> all-reduce p.q
-//   S1  x += alpha p, r -= alpha q, partial r.r
-//       and r.z with z = r / max(|aP|, SMALL)      -> all-reduce (r.r, r.z)
-//   S2  p = z + beta p                             -> barrier
+// an iteration is two phases, each closed by a group all-reduce:
+//   A  p_new = z + beta p_old (own cells into the other p buffer; the six
+//      neighbours' p_new recomputed from their stored z and p_old),
+//      q = A p_new, partial p.q                    -> all-reduce p.q
+//   B  x += alpha p, r -= alpha q, z = r / max(|aP|, SMALL) stored,
+//      partial r.r and r.z                         -> all-reduce (r.r, r.z)
 // The scalar recurrences (alpha, beta, residual, exit tests) are evaluated
 // redundantly and bit-identically by every block.
 #include <math.h>
@@ -36,7 +37,8 @@ MeshDims make_dims(int nr, int nth, int nz) {
 
 namespace {
 
-constexpr int kUnroll = 4;
+constexpr int kUnroll = 2;   // cells per thread per round (streaming phases)
+constexpr int kUnrollA = 1;  // cells per thread per round (stencil phase)
 constexpr int kMaxBlock = 1024;
 
 struct CgArgs {
@@ -48,6 +50,13 @@ struct CgArgs {
   uint64_t timeout_ns;
 };
 
+// Loops over this thread's cells of the block slice in rounds of U cells
+// (cell c0 + u*B of round c0). Every round first loads what all U cells need
+// (indices clamped into the slice, so no branch guards a load and all loads
+// of the round are in flight together), then computes and stores with the
+// out-of-slice lanes masked. Dead lanes add +0.0 to the dot sums, which
+// leaves them bit-identical to sums over the live cells alone.
+
 template <bool SYM>
 __device__ void cg_body(const CgArgs& a, Group& g) {
   const MeshDims& d = a.d;
@@ -58,21 +67,36 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
   const double* __restrict__ b = s.b;
   double* __restrict__ x = s.x;
   double* __restrict__ r = s.r;
-  double* __restrict__ p = s.p;
+  double* __restrict__ z = s.z;
   double* __restrict__ q = s.q;
-#define EAF_OWN_CELLS(...) EAF_FOR_OWN(own, kUnroll, c, __VA_ARGS__)
+  const int B = blockDim.x;
+  const int last = own.end - 1;
 
   // Preamble (src/mod_solver_3d.f90:515-530): ||Su||, z = r/max(|aP|,SMALL),
   // pv = z, r.z and r.r in one pass.
   double v3[3] = {0.0, 0.0, 0.0};
-  EAF_OWN_CELLS({
-    const double bv = b[c], rv = r[c];
-    const double z = rv / guard_small(fabs(aP[c]));
-    p[c] = z;
-    v3[0] = v3[0] + bv * bv;
-    v3[1] = v3[1] + rv * rv;
-    v3[2] = v3[2] + rv * z;
-  })
+  {
+    double* __restrict__ p0 = s.p;
+    for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnroll) {
+      double bv[kUnroll], rv[kUnroll], dv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int c = min(c0 + u * B, last);
+        bv[u] = b[c];
+        rv[u] = r[c];
+        dv[u] = aP[c];
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const bool live = c0 + u * B < own.end;
+        const double zv = rv[u] / guard_small(fabs(dv[u]));
+        if (live) p0[c0 + u * B] = zv;
+        v3[0] = v3[0] + (live ? bv[u] * bv[u] : 0.0);
+        v3[1] = v3[1] + (live ? rv[u] * rv[u] : 0.0);
+        v3[2] = v3[2] + (live ? rv[u] * zv : 0.0);
+      }
+    }
+  }
   bool ok = group_allsum<3>(v3, g, 0);
   const double bnorm = sqrt(v3[0]);
   double residual = 0.0;
@@ -80,32 +104,90 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
   bool nan_fill = false;
   if (ok && !(bnorm < kSmall)) {
     double rz = v3[2];
+    double beta = 0.0;
     residual = sqrt(v3[1]) / bnorm;
     if (residual != residual && a.max_iter >= 1) nan_fill = true;
     for (int iter = 1; iter <= a.max_iter && !nan_fill; ++iter) {
-      // S0: q = A p, p.q  (src/mod_solver_3d.f90:533-536)
+      // Phase A: pv = z + beta pv (src/mod_solver_3d.f90:556-558) fused with
+      // q = A pv and p.q (:533-534). The new direction goes to the other
+      // buffer; neighbours' new values are formed here from their stored z
+      // and old direction (both final since the last barrier), so no
+      // barrier separates the update from the stencil. Iteration 1 uses
+      // pv = z from the preamble as is.
+      const double* __restrict__ pold = (iter & 1) ? s.p2 : s.p;
+      double* __restrict__ pcur = (iter & 1) ? s.p : s.p2;
       double v1[1] = {0.0};
-      EAF_OWN_CELLS({
-        const double qv = apply_row<SYM, double>(d, A, p, c);
-        q[c] = qv;
-        v1[0] = v1[0] + p[c] * qv;
-      })
+      if (iter == 1) {
+        for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnrollA) {
+          double qv[kUnrollA], pc[kUnrollA];
+#pragma unroll
+          for (int u = 0; u < kUnrollA; ++u) {
+            const int c = min(c0 + u * B, last);
+            pc[u] = pcur[c];
+            qv[u] = apply_row<SYM, double>(d, A, pcur, c);
+          }
+#pragma unroll
+          for (int u = 0; u < kUnrollA; ++u) {
+            const bool live = c0 + u * B < own.end;
+            if (live) q[c0 + u * B] = qv[u];
+            v1[0] = v1[0] + (live ? pc[u] * qv[u] : 0.0);
+          }
+        }
+      } else {
+        const double bt = beta;
+        auto pnew = [z, pold, bt](int cc) { return z[cc] + bt * pold[cc]; };
+        for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnrollA) {
+          double qv[kUnrollA], pc[kUnrollA];
+#pragma unroll
+          for (int u = 0; u < kUnrollA; ++u) {
+            const int c = min(c0 + u * B, last);
+            pc[u] = pnew(c);
+            qv[u] = apply_row_with<SYM, double>(d, A, pc[u], pnew, c);
+          }
+#pragma unroll
+          for (int u = 0; u < kUnrollA; ++u) {
+            const bool live = c0 + u * B < own.end;
+            if (live) {
+              pcur[c0 + u * B] = pc[u];
+              q[c0 + u * B] = qv[u];
+            }
+            v1[0] = v1[0] + (live ? pc[u] * qv[u] : 0.0);
+          }
+        }
+      }
       if (!(ok = group_allsum<1>(v1, g, 3))) break;
       const double pq = v1[0];
       if (fabs(pq) < kSmall) break;
       const double alpha = rz / pq;
-      // S1: phi += alpha pv; r -= alpha q; r.r; z and r.z (:538-553)
+      // Phase B: phi += alpha pv; r -= alpha q; r.r; z and r.z (:538-553)
       double v2[2] = {0.0, 0.0};
-      EAF_OWN_CELLS({
-        const double pv = p[c], qv = q[c], dv = aP[c];
-        const double xv = x[c] + alpha * pv;
-        const double rv = r[c] - alpha * qv;
-        x[c] = xv;
-        r[c] = rv;
-        const double z = rv / guard_small(fabs(dv));
-        v2[0] = v2[0] + rv * rv;
-        v2[1] = v2[1] + rv * z;
-      })
+      for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnroll) {
+        double pv[kUnroll], qv[kUnroll], dv[kUnroll], xv[kUnroll], rv[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          const int c = min(c0 + u * B, last);
+          pv[u] = pcur[c];
+          qv[u] = q[c];
+          dv[u] = aP[c];
+          xv[u] = x[c];
+          rv[u] = r[c];
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          const bool live = c0 + u * B < own.end;
+          const double xn = xv[u] + alpha * pv[u];
+          const double rn = rv[u] - alpha * qv[u];
+          const double zv = rn / guard_small(fabs(dv[u]));
+          if (live) {
+            const int c = c0 + u * B;
+            x[c] = xn;
+            r[c] = rn;
+            z[c] = zv;
+          }
+          v2[0] = v2[0] + (live ? rn * rn : 0.0);
+          v2[1] = v2[1] + (live ? rn * zv : 0.0);
+        }
+      }
       if (!(ok = group_allsum<2>(v2, g, 4))) break;
       residual = sqrt(v2[0]) / bnorm;
       n_iter = iter;
@@ -114,23 +196,16 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
       // next direction and every later iterate are NaN in every cell, and it
       // runs to max_iter. Produce that outcome directly.
       if (residual != residual && iter < a.max_iter) { nan_fill = true; break; }
-      const double beta = v2[1] / guard_small(rz);
+      beta = v2[1] / guard_small(rz);
       rz = v2[1];
-      // S2: pv = z + beta pv (:556-558)
-      EAF_OWN_CELLS({
-        const double z = r[c] / guard_small(fabs(aP[c]));
-        p[c] = z + beta * p[c];
-      })
-      if (!(ok = group_barrier(g))) break;
     }
     if (nan_fill) {
       const double qnan = __longlong_as_double(0x7ff8000000000000ll);
-      EAF_OWN_CELLS({ x[c] = qnan; })
+      for (int c = own.begin + (int)threadIdx.x; c < own.end; c += B) x[c] = qnan;
       residual = qnan;
       n_iter = a.max_iter;
     }
   }
-#undef EAF_OWN_CELLS
   if (g.bid == 0 && threadIdx.x == 0) {
     SolveResult* res = a.ws.result;
     const int err = ld_volatile_i32(a.ws.err);
@@ -148,6 +223,7 @@ __global__ void __launch_bounds__(kMaxBlock) cg_f64_kernel(CgArgs a) {
   g.counter = a.ws.counter;
   g.err = a.ws.err;
   g.part = a.ws.part;
+  g.stage = group_stage_smem();
   g.nb = gridDim.x;
   g.bid = blockIdx.x;
   g.timeout_ns = a.timeout_ns;
@@ -308,5 +384,7 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
 }
 
 const void* cg_f64_kernel_ptr() { return (const void*)cg_f64_kernel; }
+
+
 
 }  // namespace eaf

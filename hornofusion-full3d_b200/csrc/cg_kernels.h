@@ -36,7 +36,9 @@ struct HaloInputs {
 struct SysF64 {
   double *aP, *aE, *aN, *aT;  // symmetric form: aW, aS, aB are implied
   double *aW, *aS, *aB;       // general form only
-  double *b, *x, *r, *p, *q;
+  double *b, *x, *r, *q;
+  double *p, *p2;             // search direction, double-buffered by iteration
+  double *z;                  // preconditioned residual r / max(|aP|, SMALL)
   int* asym;                  // pack: number of link pairs that disagree
 };
 
@@ -69,6 +71,8 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
                           int max_iter, double tol, uint64_t timeout_ns,
                           int grid, int block, cudaStream_t st);
 const void* cg_f64_kernel_ptr();
+
+
 
 // Mixed precision (cg_mixed.cu).
 cudaError_t launch_cg_mixed(const MeshDims& d, const SysF64& s, const SysF32& f,

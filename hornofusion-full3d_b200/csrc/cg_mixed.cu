@@ -181,6 +181,7 @@ __global__ void __launch_bounds__(kMaxBlock) cg_mixed_kernel(MixArgs a) {
   g.counter = a.ws.counter;
   g.err = a.ws.err;
   g.part = a.ws.part;
+  g.stage = group_stage_smem();
   g.nb = gridDim.x;
   g.bid = blockIdx.x;
   g.timeout_ns = a.timeout_ns;

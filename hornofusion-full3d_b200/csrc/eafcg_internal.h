@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+
 namespace eaf {
 
 // Records the last CUDA failure of this thread for eaf_last_error().
@@ -22,5 +23,6 @@ class DeviceGuard {
   int prev_;
   bool ok_;
 };
+
 
 }  // namespace eaf

@@ -45,10 +45,10 @@ constexpr int kMaxDevices = 64;
 constexpr uint64_t kNoallocTimeoutNs = 2000ull * 1000ull * 1000ull;
 
 // Scratch layout (doubles unless stated):
-//   12 compact arrays of kNoallocMaxCells: aP aE aN aT aW aS aB b x r p q
+//   14 compact arrays of kNoallocMaxCells: aP aE aN aT aW aS aB b x r p q p2 z
 //   partial table: kPartSlots * kNoallocMaxBlocks
 //   barrier counter (u64), error word (int), symmetry flag (int), result
-constexpr size_t kArrays = 12;
+constexpr size_t kArrays = 14;
 constexpr size_t kPartOff = kArrays * kNoallocMaxCells;
 constexpr size_t kCounterOff = kPartOff + (size_t)kPartSlots * kNoallocMaxBlocks;
 constexpr size_t kErrOff = kCounterOff + 1;    // one double slot each
@@ -137,6 +137,8 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
   s.r = base + 9 * M;
   s.p = base + 10 * M;
   s.q = base + 11 * M;
+  s.p2 = base + 12 * M;
+  s.z = base + 13 * M;
   s.asym = reinterpret_cast<int*>(base + kAsymOff);
   eaf::GroupWs ws;
   ws.part = base + kPartOff;
@@ -146,7 +148,8 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
 
   // Launch shape: the default of eaf_cg_create handles (one 1024-thread
   // block up to 8192 cells, else one 512-thread block per 2048 cells),
-  // capped by co-residency and by the partial table's kNoallocMaxBlocks.
+  // capped by co-residency, so that results match the handle entry points
+  // bit for bit.
   int block = 512, grid;
   if (n <= 8192) {
     block = 1024;

@@ -18,39 +18,47 @@ struct Coefs {
 };
 
 // y = A x at compact cell c in the expression order of the reference matvec
+// (x at c given as xc, at the neighbours produced by xv(cell))
 // (src/mod_solver_3d.f90:597-603): aP*x - aW*xW - aE*xE - aS*xS - aN*xN
 // - aB*xB - aT*xT. In the symmetric form aW(c) = aE(c-1), aS(c) =
 // aN(south of c) and aB(c) = aT(c-plane); the wall links of a symmetric
 // operator are zero and the reference's Krylov vectors are zero in their r/z
 // halos, so the wall terms skipped here are exact zeros there too.
-template <bool SYM, typename T>
-__device__ __forceinline__ T apply_row(const MeshDims& d, const Coefs<T>& A,
-                                       const T* __restrict__ x, int c) {
+template <bool SYM, typename T, typename XF>
+__device__ __forceinline__ T apply_row_with(const MeshDims& d, const Coefs<T>& A, T xc,
+                                            XF xv, int c) {
   int i, j, k;
   cell_ijk(d, c, i, j, k);
   const int cs = j > 0 ? c - d.nr : c + (d.nth - 1) * d.nr;
   const int cn = j < d.nth - 1 ? c + d.nr : c - (d.nth - 1) * d.nr;
-  T y = A.aP[c] * x[c];
+  T y = A.aP[c] * xc;
   if (SYM) {
-    if (i > 0) y = y - A.aE[c - 1] * x[c - 1];
-    if (i < d.nr - 1) y = y - A.aE[c] * x[c + 1];
-    y = y - A.aN[cs] * x[cs];
-    y = y - A.aN[c] * x[cn];
-    if (k > 0) y = y - A.aT[c - d.plane] * x[c - d.plane];
-    if (k < d.nz - 1) y = y - A.aT[c] * x[c + d.plane];
+    if (i > 0) y = y - A.aE[c - 1] * xv(c - 1);
+    if (i < d.nr - 1) y = y - A.aE[c] * xv(c + 1);
+    y = y - A.aN[cs] * xv(cs);
+    y = y - A.aN[c] * xv(cn);
+    if (k > 0) y = y - A.aT[c - d.plane] * xv(c - d.plane);
+    if (k < d.nz - 1) y = y - A.aT[c] * xv(c + d.plane);
   } else {
-    const T xw = i > 0 ? x[c - 1] : T(0);
-    const T xe = i < d.nr - 1 ? x[c + 1] : T(0);
-    const T xb = k > 0 ? x[c - d.plane] : T(0);
-    const T xt = k < d.nz - 1 ? x[c + d.plane] : T(0);
+    const T xw = i > 0 ? xv(c - 1) : T(0);
+    const T xe = i < d.nr - 1 ? xv(c + 1) : T(0);
+    const T xb = k > 0 ? xv(c - d.plane) : T(0);
+    const T xt = k < d.nz - 1 ? xv(c + d.plane) : T(0);
     y = y - A.aW[c] * xw;
     y = y - A.aE[c] * xe;
-    y = y - A.aS[c] * x[cs];
-    y = y - A.aN[c] * x[cn];
+    y = y - A.aS[c] * xv(cs);
+    y = y - A.aN[c] * xv(cn);
     y = y - A.aB[c] * xb;
     y = y - A.aT[c] * xt;
   }
   return y;
+}
+
+// The operator applied to a stored vector x.
+template <bool SYM, typename T>
+__device__ __forceinline__ T apply_row(const MeshDims& d, const Coefs<T>& A,
+                                       const T* __restrict__ x, int c) {
+  return apply_row_with<SYM, T>(d, A, x[c], [x](int cc) { return x[cc]; }, c);
 }
 
 template <typename T>

@@ -124,6 +124,10 @@ int eaf_cg_solve_mixed_device(eaf_cg_t h, const double* aW, const double* aE,
 int eaf_cg_set_launch(eaf_cg_t h, int block_threads, int grid_blocks);
 int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks);
 
+/* Launch shape of the last solve (it fixes the association of the device
+ * dot products; the oracle's kernel-order mode takes the same shape). */
+int eaf_cg_last_launch(eaf_cg_t h, int* block_threads, int* grid_blocks);
+
 /* Bound on every device-side barrier wait, in milliseconds (default 2000). */
 int eaf_cg_set_timeout_ms(eaf_cg_t h, double ms);
 
@@ -155,7 +159,7 @@ int eaf_host_unregister(void* ptr);
  * cudaMalloc/cudaFree would synchronise the device. Same contract and
  * result as eaf_cg_solve_f64_device (device pointers, reference layout),
  * but without a handle: all working memory is one static device array of
- * EAF_NOALLOC_MAX_CELLS cells' worth (about 3 MiB) that every GPU loading
+ * EAF_NOALLOC_MAX_CELLS cells' worth (about 3.5 MiB) that every GPU loading
  * the library holds until process exit. Larger meshes return EAF_EINVAL
  * (see eaf_last_error()). The array is shared by all calls on a device and
  * keeps the last call's contents; calls whose GPU work overlaps on one
@@ -177,6 +181,14 @@ int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device, void* stream,
  * must return EAF_ETIMEOUT after about timeout_ms, with the device context
  * intact. No reference counterpart (failure-detection test hook). */
 int eaf_selftest_barrier_timeout(int device, double timeout_ms);
+
+/* Diagnostics (no reference counterpart): device time of one group
+ * all-reduce of two sums -- block reduction, bounded group barrier, staging
+ * and fold of the block partials -- averaged over `iters` in one cooperative
+ * launch of blocks x threads, with barrier memory-ordering form 0, 1 or 2
+ * (the solvers use form 1). */
+int eaf_diag_allreduce_us(int device, int blocks, int threads, int iters,
+                          int form, double* us_per_allreduce);
 
 /* Library version string. */
 const char* eaf_version(void);

@@ -331,8 +331,9 @@ int eaf_oracle_cg(int nr, int nth, int nz, const double* aW, const double* aE,
 }
 
 /* The same restatement with the dot products associated as the CUDA kernels
- * associate them for a launch of G blocks x B threads: every other operation
- * is unchanged, so a CUDA solve launched that way must agree bit for bit. */
+ * associate them for a launch of G blocks x B threads (block g owns the g-th
+ * contiguous slice of ceil(n/G) cells): every other operation is unchanged,
+ * so a CUDA solve launched that way must agree bit for bit. */
 int eaf_oracle_cg_tree(int nr, int nth, int nz, const double* aW,
                        const double* aE, const double* aS, const double* aN,
                        const double* aB, const double* aT, const double* aP,

@@ -38,17 +38,19 @@ def rel_l2(a, b):
 
 
 def gpu_solve(s, phi, max_iter=200000, tol=TOL, launch=None):
+    """Solve through the C ABI; returns the oracle plan (grid, block) the
+    solve ran with. launch=(block, grid) sets the launch shape (0 = auto)."""
     eaf = pkg()
     with eaf.CGSolver(s.nr, s.nth, s.nz) as cg:
         if launch is not None:
             cg.set_launch(*launch)
-        block, grid = cg.launch()
         res, nit, st = cg.solve(s.arrays(), phi, max_iter, tol)
         timing = cg.last_timing()
-    return res, nit, st, (grid, block), timing
+        plan = cg.last_launch()
+    return res, nit, st, plan, timing
 
 
-def assert_bitwise(s, phi0, max_iter=200000, tol=TOL, launch=None, orc=None):
+def assert_bitwise(s, phi0, max_iter=200000, tol=TOL, launch=None):
     import oracle
     phi_g = phi0.copy()
     res_g, nit_g, st, plan, timing = gpu_solve(s, phi_g, max_iter, tol, launch)
@@ -91,12 +93,13 @@ def test_mid_meshes_bitwise_kernel_order(dims):
     assert st == 0 and res < TOL
 
 
-def test_production_mesh_fixed_iterations_bitwise():
+@pytest.mark.parametrize("launch", [None, (1024, 148)])
+def test_production_mesh_fixed_iterations_bitwise(launch):
     """60x120x84, 150 iterations with tol 0: kernel-order bitwise."""
     g = gen()
     s = g.make_system(*g.PRODUCTION, seed=0)
     res, nit, st, plan, _ = assert_bitwise(s, g.zeros_phi(60, 120, 84),
-                                           max_iter=150, tol=0.0)
+                                           max_iter=150, tol=0.0, launch=launch)
     assert nit == 150 and plan[0] > 1
 
 
@@ -148,13 +151,14 @@ def test_general_form_nonzero_wall_link_reads_phi_halo():
 
 @pytest.mark.parametrize("dims", [(1, 1, 1), (2, 1, 3), (3, 2, 2), (1, 5, 4),
                                   (4, 3, 1), (5, 7, 6)])
-def test_tiny_meshes_bitwise(dims):
+@pytest.mark.parametrize("launch", [None, (64, 3)])
+def test_tiny_meshes_bitwise(dims, launch):
     g = gen()
     nr, nth, nz = dims
     s = g.make_system(nr, nth, nz, nsph=2, seed=7)
     rng = np.random.default_rng(1)
     g.interior(s.Su)[...] = rng.normal(0, 1e-3, size=(nz, nth, nr))
-    assert_bitwise(s, g.zeros_phi(nr, nth, nz), max_iter=500)
+    assert_bitwise(s, g.zeros_phi(nr, nth, nz), max_iter=500, launch=launch)
 
 
 def test_zero_rhs_early_return():
