@@ -28,7 +28,7 @@ from ._lib import (EAF_EBUSY, EAF_ENONFINITE, EAF_ETIMEOUT, EAF_OK, EafError,
 SOR_TOL_PRESSURE = 1.0e-8     # src/mod_constants.f90:143
 MAX_INNER_PRES = 50           # src/mod_config_3d.f90:41 (default cap)
 
-__all__ = ["CGSolver", "cg_3d", "EafError", "load", "SOR_TOL_PRESSURE",
+__all__ = ["CGSolver", "Batch", "cg_3d", "EafError", "load", "SOR_TOL_PRESSURE",
            "MAX_INNER_PRES", "halo_shape"]
 
 
@@ -152,6 +152,79 @@ class CGSolver:
     @property
     def stream(self) -> int:
         return self._lib.eaf_cg_stream(self._h) or 0
+
+
+class Batch:
+    """Many independent systems solved in one persistent launch (C ABI
+    eaf_batch_*). ``dims`` is a list of (nr, nth, nz)."""
+
+    def __init__(self, dims, device: int = 0):
+        self._lib = load()
+        self.dims = [tuple(int(v) for v in d) for d in dims]
+        flat = (ctypes.c_int * (3 * len(self.dims)))(*[v for d in self.dims for v in d])
+        h = ctypes.c_void_p()
+        check(self._lib.eaf_batch_create(ctypes.byref(h), len(self.dims), flat, device),
+              "eaf_batch_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.eaf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_width(self, sys: int, width: int) -> None:
+        check(self._lib.eaf_batch_set_width(self._h, sys, width), "set_width")
+
+    def lane_width(self, sys: int) -> int:
+        w = ctypes.c_int()
+        check(self._lib.eaf_batch_lane_width(self._h, sys, ctypes.byref(w)))
+        return w.value
+
+    def plan(self) -> tuple:
+        g, b, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._lib.eaf_batch_plan(self._h, ctypes.byref(g), ctypes.byref(b),
+                                       ctypes.byref(n)), "eaf_batch_plan")
+        return g.value, b.value, n.value
+
+    def set_system(self, sys: int, arrays, phi, device_ptrs: bool = False) -> None:
+        arrays = list(arrays)
+        fn = (self._lib.eaf_batch_set_system_device if device_ptrs
+              else self._lib.eaf_batch_set_system)
+        check(fn(self._h, sys, *[_ptr(a) for a in arrays], _ptr(phi)),
+              "eaf_batch_set_system")
+
+    def solve(self, mixed: bool = False, max_iter: int = 200000,
+              tol: float = SOR_TOL_PRESSURE, max_outer: int = 60,
+              inner_tol: float = 0.1) -> int:
+        st = self._lib.eaf_batch_solve(self._h, int(bool(mixed)), int(max_iter),
+                                       float(tol), int(max_outer), float(inner_tol))
+        return check(st, "eaf_batch_solve", allow=(EAF_OK, EAF_ENONFINITE))
+
+    def result(self, sys: int) -> tuple:
+        r, n, o, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._lib.eaf_batch_result(self._h, sys, ctypes.byref(r), ctypes.byref(n),
+                                         ctypes.byref(o), ctypes.byref(st)))
+        return r.value, n.value, o.value, st.value
+
+    def get_phi(self, sys: int, out: np.ndarray) -> np.ndarray:
+        check(self._lib.eaf_batch_get_phi(self._h, sys, _ptr(out)), "eaf_batch_get_phi")
+        return out
+
+    @property
+    def last_ms(self) -> float:
+        return self._lib.eaf_batch_last_ms(self._h)
 
 
 _solvers: dict = {}

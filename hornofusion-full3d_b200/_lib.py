@@ -61,6 +61,18 @@ SIGNATURES = [
     ("eaf_host_unregister", _ci, [_vp]),
     ("eaf_selftest_barrier_timeout", _ci, [_ci, _cd]),
     ("eaf_diag_allreduce_us", _ci, [_ci, _ci, _ci, _ci, _ci, _pd]),
+    ("eaf_batch_create", _ci, [ctypes.POINTER(_vp), _ci, _pi, _ci]),
+    ("eaf_batch_destroy", _ci, [_vp]),
+    ("eaf_batch_set_width", _ci, [_vp, _ci, _ci]),
+    ("eaf_batch_lane_width", _ci, [_vp, _ci, _pi]),
+    ("eaf_batch_plan", _ci, [_vp, _pi, _pi, _pi]),
+    ("eaf_batch_set_system", _ci, [_vp, _ci] + [_vp] * 9),
+    ("eaf_batch_set_system_device", _ci, [_vp, _ci] + [_vp] * 9),
+    ("eaf_batch_solve", _ci, [_vp, _ci, _ci, _cd, _ci, _cd]),
+    ("eaf_batch_result", _ci, [_vp, _ci, _pd, _pi, _pi, _pi]),
+    ("eaf_batch_get_phi", _ci, [_vp, _ci, _vp]),
+    ("eaf_batch_last_ms", _cd, [_vp]),
+    ("eaf_batch_stream", _vp, [_vp]),
     ("eaf_cg_solve_f64_noalloc", _ci,
      [_ci, _ci, _ci, _ci, _vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
 ]

@@ -32,7 +32,7 @@ UNITS = {
     "api.cu": [],
     "cg_f64.cu": ["-fmad=false"],
     "cg_mixed.cu": [],
-    "cg_batch.cu": [],
+    "batch.cu": [],
     "noalloc.cu": ["-fmad=false"],
     "serve.cu": [],
     "diag.cu": [],

@@ -88,7 +88,7 @@ static void free_handle(eaf_cg* h) {
   for (double* p : f64) cudaFree(p);
   cudaFree(h->s.asym);
   float* f32[] = {h->f.aP, h->f.aE, h->f.aN, h->f.aT, h->f.aW, h->f.aS, h->f.aB,
-                  h->f.r,  h->f.p,  h->f.q,  h->f.e};
+                  h->f.r,  h->f.z,  h->f.q,  h->f.e,  h->f.p,  h->f.p2};
   for (float* p : f32) cudaFree(p);
   cudaFree(h->ws.part);
   cudaFree(h->ws.counter);
@@ -306,8 +306,9 @@ bool any_null(const double* const* p, int n) {
 int ensure_f32(eaf_cg* h) {
   if (h->have_f32) return EAF_OK;
   const size_t n = (size_t)h->d.n;
-  float** f32[] = {&h->f.aP, &h->f.aE, &h->f.aN, &h->f.aT, &h->f.aW, &h->f.aS,
-                   &h->f.aB, &h->f.r,  &h->f.p,  &h->f.q,  &h->f.e};
+  float** f32[] = {&h->f.aP, &h->f.aE, &h->f.aN, &h->f.aT, &h->f.aW,
+                   &h->f.aS, &h->f.aB, &h->f.r,  &h->f.z,  &h->f.q,
+                   &h->f.e,  &h->f.p,  &h->f.p2};
   for (float** p : f32) {
     cudaError_t e = cudaMalloc((void**)p, n * sizeof(float));
     if (e != cudaSuccess) {

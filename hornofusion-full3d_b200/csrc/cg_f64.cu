@@ -235,6 +235,49 @@ __global__ void __launch_bounds__(kMaxBlock) cg_f64_kernel(CgArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Batched launch (see BatchTables): the same solver body per system, on the
+// lane's blocks with the lane's barrier counter and partial table.
+// ---------------------------------------------------------------------------
+struct BatchF64Args {
+  BatchTables t;
+  int max_iter;
+  double tol;
+  uint64_t timeout_ns;
+};
+
+__global__ void __launch_bounds__(kMaxBlock) batch_f64_kernel(BatchF64Args a) {
+  const int lane = a.t.lane_of_block[blockIdx.x];
+  const int first = a.t.lane_first_block[lane];
+  Group g;
+  g.counter = a.t.counters + (size_t)lane * kCounterStride;
+  g.err = a.t.err;
+  g.part = a.t.parts + (size_t)8 * first;
+  g.stage = group_stage_smem();
+  g.nb = a.t.lane_width[lane];
+  g.bid = blockIdx.x - first;
+  g.timeout_ns = a.timeout_ns;
+  g.epoch = 0;
+  for (int qi = a.t.lane_q_begin[lane]; qi < a.t.lane_q_begin[lane + 1]; ++qi) {
+    if (ld_volatile_i32(a.t.err) != 0) break;
+    const BatchSys& bs = a.t.sys[a.t.queue[qi]];
+    CgArgs ca;
+    ca.d = bs.d;
+    ca.s = bs.s;
+    ca.ws.part = g.part;
+    ca.ws.counter = g.counter;
+    ca.ws.err = a.t.err;
+    ca.ws.result = bs.result;
+    ca.max_iter = a.max_iter;
+    ca.tol = a.tol;
+    ca.timeout_ns = a.timeout_ns;
+    if (*bs.s.asym == 0)
+      cg_body<true>(ca, g);
+    else
+      cg_body<false>(ca, g);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // pack / unpack
 // ---------------------------------------------------------------------------
 struct PackArgs {
@@ -338,6 +381,7 @@ cudaError_t launch_pack_f64(const MeshDims& d, const HaloInputs& in, const SysF6
   a.s = s;
   a.hy = d.nr + 4;
   a.hz = (long long)(d.nr + 4) * (d.nth + 4);
+  (void)cudaGetLastError();  // report this launch's error, not an older one
   cudaError_t e = cudaMemsetAsync(s.asym, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   const int block = 256;
@@ -358,6 +402,7 @@ cudaError_t launch_unpack_f64(const MeshDims& d, const double* x, double* phi,
   a.fd_hy = FastDiv((uint32_t)a.hy);
   a.fd_hj = FastDiv((uint32_t)a.hj);
   a.total = (long long)(d.nr + 4) * (d.nth + 4) * (d.nz + 4);
+  (void)cudaGetLastError();  // report this launch's error, not an older one
   const int block = 256;
   long long g = (a.total + block - 1) / block;
   int grid = (int)(g > 148 * 16 ? 148 * 16 : g);
@@ -384,6 +429,28 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
 }
 
 const void* cg_f64_kernel_ptr() { return (const void*)cg_f64_kernel; }
+
+cudaError_t launch_batch_f64(const BatchTables& t, int grid, int block, int max_iter,
+                             double tol, uint64_t timeout_ns, cudaStream_t st) {
+  BatchF64Args a;
+  a.t = t;
+  a.max_iter = max_iter;
+  a.tol = tol;
+  a.timeout_ns = timeout_ns;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, batch_f64_kernel, a);
+}
+
+const void* batch_f64_kernel_ptr() { return (const void*)batch_f64_kernel; }
 
 
 

@@ -45,7 +45,8 @@ struct SysF64 {
 // FP32 shadow of a system for the mixed-precision inner solve.
 struct SysF32 {
   float *aP, *aE, *aN, *aT, *aW, *aS, *aB;
-  float *r, *p, *q, *e;  // inner residual, direction, A p, correction
+  float *r, *z, *q, *e;  // inner residual, r / max(|aP|, SMALL), A p, correction
+  float *p, *p2;         // direction, double-buffered by inner iteration
 };
 
 struct GroupWs {
@@ -80,6 +81,41 @@ cudaError_t launch_cg_mixed(const MeshDims& d, const SysF64& s, const SysF32& f,
                             double tol, double inner_tol, uint64_t timeout_ns,
                             int grid, int block, cudaStream_t st);
 const void* cg_mixed_kernel_ptr();
+
+// ---------------------------------------------------------------------------
+// Batched launch: independent systems, one persistent cooperative launch.
+// Blocks are split into lanes of consecutive blocks; a lane solves the
+// systems of its queue one after another with a lane-local group barrier.
+// A system's reduction order depends only on its lane width and the block
+// size, never on the rest of the batch.
+// ---------------------------------------------------------------------------
+struct BatchSys {
+  MeshDims d;
+  SysF64 s;
+  SysF32 f;
+  SolveResult* result;
+};
+
+struct BatchTables {
+  const BatchSys* sys;          // [nsys]
+  const int* lane_of_block;     // [grid]
+  const int* lane_first_block;  // [nlanes]
+  const int* lane_width;        // [nlanes]
+  const int* lane_q_begin;      // [nlanes + 1], offsets into queue
+  const int* queue;             // system ids, lane by lane
+  unsigned long long* counters; // [nlanes * kCounterStride]
+  double* parts;                // [8 * grid]: lane L uses [8*first, 8*(first+width))
+  int* err;                     // shared error word
+};
+constexpr int kCounterStride = 16;  // 128 bytes between lane counters
+
+cudaError_t launch_batch_f64(const BatchTables& t, int grid, int block, int max_iter,
+                             double tol, uint64_t timeout_ns, cudaStream_t st);
+cudaError_t launch_batch_mixed(const BatchTables& t, int grid, int block,
+                               int max_outer, int max_inner, double tol,
+                               double inner_tol, uint64_t timeout_ns, cudaStream_t st);
+const void* batch_f64_kernel_ptr();
+const void* batch_mixed_kernel_ptr();
 
 // Barrier self-test (api.cu).
 cudaError_t launch_barrier_selftest(const GroupWs& ws, uint64_t timeout_ns,

@@ -152,6 +152,49 @@ int eaf_host_free(void* ptr);
 int eaf_host_register(void* ptr, size_t bytes);
 int eaf_host_unregister(void* ptr);
 
+/* ---- batched solves ------------------------------------------------------ */
+/* No reference counterpart: many independent pressure systems of uneven
+ * mesh size solved in ONE persistent cooperative launch, replayed from a
+ * CUDA graph. Each system is solved on a lane of blocks whose width depends
+ * only on its mesh size (tuned table, or eaf_batch_set_width), so its
+ * result is bit-identical whatever else is in the batch. Array contract per
+ * system: that of eaf_cg_solve_f64. */
+typedef struct eaf_batch* eaf_batch_t;
+/* dims: 3*nsys ints, (nr, nth, nz) per system. Allocates all device state. */
+int eaf_batch_create(eaf_batch_t* out, int nsys, const int* dims, int device);
+int eaf_batch_destroy(eaf_batch_t b);
+/* Lane width override for one system (0 = tuned width); replans. */
+int eaf_batch_set_width(eaf_batch_t b, int sys, int width);
+int eaf_batch_lane_width(eaf_batch_t b, int sys, int* width);
+/* Plans lanes and queues (done by the first solve otherwise). */
+int eaf_batch_plan(eaf_batch_t b, int* grid, int* block, int* nlanes);
+/* Host inputs of one system, uploaded on the batch stream (phi is the
+ * warm start and, after a solve, is read back with eaf_batch_get_phi). */
+int eaf_batch_set_system(eaf_batch_t b, int sys, const double* aW,
+                         const double* aE, const double* aS, const double* aN,
+                         const double* aB, const double* aT, const double* aP,
+                         const double* Su, const double* phi);
+/* Device inputs of one system: read in place by every later solve; phi is
+ * updated in place. */
+int eaf_batch_set_system_device(eaf_batch_t b, int sys, const double* aW,
+                                const double* aE, const double* aS,
+                                const double* aN, const double* aB,
+                                const double* aT, const double* aP,
+                                const double* Su, double* phi);
+/* Solves every system: plain FP64 (mixed = 0; max_iter, tol as
+ * eaf_cg_solve_f64) or mixed (mixed = 1; max_iter = inner iterations per
+ * refinement step, max_outer refinement steps, inner_tol as
+ * eaf_cg_solve_mixed). Returns EAF_OK, or the first non-OK system status
+ * (EAF_ETIMEOUT first). */
+int eaf_batch_solve(eaf_batch_t b, int mixed, int max_iter, double tol,
+                    int max_outer, double inner_tol);
+int eaf_batch_result(eaf_batch_t b, int sys, double* residual, int* n_iter,
+                     int* n_outer, int* status);
+int eaf_batch_get_phi(eaf_batch_t b, int sys, double* phi);
+/* Device time of the last solve's persistent launch, milliseconds. */
+double eaf_batch_last_ms(eaf_batch_t b);
+void* eaf_batch_stream(eaf_batch_t b);
+
 /* ---- no-allocation entry point ----------------------------------------- */
 /* No counterpart in the reference. For callers that must not allocate
  * device memory: a simulator whose device memory is owned by its own pool
