@@ -28,7 +28,7 @@ from ._lib import (EAF_EBUSY, EAF_ENONFINITE, EAF_ETIMEOUT, EAF_OK, EafError,
 SOR_TOL_PRESSURE = 1.0e-8     # src/mod_constants.f90:143
 MAX_INNER_PRES = 50           # src/mod_config_3d.f90:41 (default cap)
 
-__all__ = ["CGSolver", "Batch", "cg_3d", "EafError", "load", "SOR_TOL_PRESSURE",
+__all__ = ["CGSolver", "Batch", "Server", "cg_3d", "EafError", "load", "SOR_TOL_PRESSURE",
            "MAX_INNER_PRES", "halo_shape"]
 
 
@@ -225,6 +225,101 @@ class Batch:
     @property
     def last_ms(self) -> float:
         return self._lib.eaf_batch_last_ms(self._h)
+
+
+class Server:
+    """The serving loop (C ABI eaf_srv_*): device-resident runs, admission
+    by HBM budget, continuous batching of their pressure solves."""
+
+    def __init__(self, device: int = 0, budget_bytes: float = 150e9,
+                 mixed: bool = False, max_iter: int = 200000,
+                 tol: float = SOR_TOL_PRESSURE, max_outer: int = 60,
+                 inner_tol: float = 0.1, max_batch: int = 128):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        check(self._lib.eaf_srv_create(ctypes.byref(h), device, float(budget_bytes),
+                                       int(bool(mixed)), int(max_iter), float(tol),
+                                       int(max_outer), float(inner_tol), int(max_batch)),
+              "eaf_srv_create")
+        self._h = h
+        # The server reads a request's inputs and writes its phi_out until the
+        # ticket completes: keep those arrays alive until then.
+        self._held: dict = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.eaf_srv_destroy(self._h)   # finishes all requests first
+            self._h = None
+            self._held.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def open_run(self, nr: int, nth: int, nz: int) -> int:
+        rid = ctypes.c_int()
+        check(self._lib.eaf_srv_open_run(self._h, nr, nth, nz, ctypes.byref(rid)),
+              "eaf_srv_open_run")
+        return rid.value
+
+    def try_open_run(self, nr: int, nth: int, nz: int):
+        """Run id, or None when the HBM budget refuses the run."""
+        rid = ctypes.c_int()
+        st = self._lib.eaf_srv_open_run(self._h, nr, nth, nz, ctypes.byref(rid))
+        if st == _lib.EAF_EADMIT:
+            return None
+        check(st, "eaf_srv_open_run")
+        return rid.value
+
+    def close_run(self, run: int) -> None:
+        check(self._lib.eaf_srv_close_run(self._h, run), "eaf_srv_close_run")
+
+    def submit(self, run: int, arrays, phi_out=None) -> int:
+        arrays = list(arrays)
+        t = ctypes.c_longlong()
+        check(self._lib.eaf_srv_submit(self._h, run, *[_ptr(a) for a in arrays],
+                                       _ptr(phi_out) if phi_out is not None else None,
+                                       ctypes.byref(t)), "eaf_srv_submit")
+        self._held[t.value] = (arrays, phi_out)
+        return t.value
+
+    def poll(self, ticket: int):
+        """None while pending, else (residual, n_iter, n_outer, status)."""
+        r, n, o, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        rc = self._lib.eaf_srv_poll(self._h, ticket, ctypes.byref(r), ctypes.byref(n),
+                                    ctypes.byref(o), ctypes.byref(st))
+        if rc == _lib.EAF_EBUSY:
+            return None
+        check(rc, "eaf_srv_poll")
+        self._held.pop(ticket, None)
+        return r.value, n.value, o.value, st.value
+
+    def wait(self, ticket: int, timeout_ms: float = 60000.0):
+        r, n, o, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._lib.eaf_srv_wait(self._h, ticket, float(timeout_ms), ctypes.byref(r),
+                                     ctypes.byref(n), ctypes.byref(o), ctypes.byref(st)),
+              "eaf_srv_wait")
+        self._held.pop(ticket, None)
+        return r.value, n.value, o.value, st.value
+
+    def stats(self) -> dict:
+        st = _lib.SrvStats()
+        check(self._lib.eaf_srv_stats(self._h, ctypes.byref(st)), "eaf_srv_stats")
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def reset_stats(self) -> None:
+        check(self._lib.eaf_srv_reset_stats(self._h))
+
+    def inject_device_lost(self) -> None:
+        check(self._lib.eaf_srv_inject_fault(self._h, _lib.EAF_FAULT_DEVICE_LOST))
 
 
 _solvers: dict = {}

@@ -22,6 +22,16 @@ EAF_EADMIT = 7
 EAF_EBUSY = 8
 EAF_ECLOSED = 9
 EAF_NOALLOC_MAX_CELLS = 32768
+EAF_FAULT_DEVICE_LOST = 1
+
+
+class SrvStats(ctypes.Structure):
+    """eaf_srv_stats_t"""
+    _fields_ = [(n, ctypes.c_longlong) for n in
+                ("solves", "batches", "admitted_runs", "refused_runs", "active_runs")] + \
+               [(n, ctypes.c_double) for n in
+                ("p50_ms", "p99_ms", "mean_ms", "max_ms", "solves_per_s",
+                 "mean_batch", "used_bytes", "budget_bytes")]
 
 STATUS_NAMES = {
     0: "EAF_OK", 1: "EAF_ECUDA", 2: "EAF_EINVAL", 3: "EAF_ENONFINITE",
@@ -73,6 +83,16 @@ SIGNATURES = [
     ("eaf_batch_get_phi", _ci, [_vp, _ci, _vp]),
     ("eaf_batch_last_ms", _cd, [_vp]),
     ("eaf_batch_stream", _vp, [_vp]),
+    ("eaf_srv_create", _ci, [ctypes.POINTER(_vp), _ci, _cd, _ci, _ci, _cd, _ci, _cd, _ci]),
+    ("eaf_srv_destroy", _ci, [_vp]),
+    ("eaf_srv_open_run", _ci, [_vp, _ci, _ci, _ci, _pi]),
+    ("eaf_srv_close_run", _ci, [_vp, _ci]),
+    ("eaf_srv_submit", _ci, [_vp, _ci] + _A8 + [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    ("eaf_srv_poll", _ci, [_vp, ctypes.c_longlong, _pd, _pi, _pi, _pi]),
+    ("eaf_srv_wait", _ci, [_vp, ctypes.c_longlong, _cd, _pd, _pi, _pi, _pi]),
+    ("eaf_srv_stats", _ci, [_vp, _vp]),
+    ("eaf_srv_reset_stats", _ci, [_vp]),
+    ("eaf_srv_inject_fault", _ci, [_vp, _ci]),
     ("eaf_cg_solve_f64_noalloc", _ci,
      [_ci, _ci, _ci, _ci, _vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
 ]

@@ -36,7 +36,7 @@ using eaf::SolveResult;
 
 namespace {
 
-constexpr int kBatchBlock = 512;
+
 
 double model_iter_us(long long cells, int w) {
   const double cpb = (double)cells / w;
@@ -45,11 +45,137 @@ double model_iter_us(long long cells, int w) {
   return 2.0 * phase + 2.0 * red;
 }
 
+}  // namespace
+
+namespace eaf {
+
 double model_solve_us(long long cells, int w) {
   return 8.0 * sqrt((double)cells) * model_iter_us(cells, w);
 }
 
-}  // namespace
+int batch_capacity(int device, int* blocks) {
+  int per_sm64 = 0, per_sm32 = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm64, batch_f64_kernel_ptr(),
+                                                    eaf::kBatchBlock, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, batch_mixed_kernel_ptr(),
+                                                    eaf::kBatchBlock, 0) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    set_error("batch: occupancy query", cudaErrorUnknown);
+    return EAF_ECUDA;
+  }
+  *blocks = std::min(std::min(per_sm64, per_sm32) * sms, kMaxGroupBlocks);
+  return EAF_OK;
+}
+
+std::vector<int> LanePlan::packed() const {
+  std::vector<int> host;
+  host.insert(host.end(), lane_of_block.begin(), lane_of_block.end());
+  host.insert(host.end(), lane_first.begin(), lane_first.end());
+  host.insert(host.end(), lane_width.begin(), lane_width.end());
+  host.insert(host.end(), q_begin.begin(), q_begin.end());
+  host.insert(host.end(), queue.begin(), queue.end());
+  return host;
+}
+
+BatchTables tables_from(const int* d_tab, int grid, int nlanes, const BatchSys* d_sys,
+                        unsigned long long* counters, double* parts, int* err) {
+  BatchTables t;
+  const int* p = d_tab;
+  t.sys = d_sys;
+  t.lane_of_block = p;
+  p += grid;
+  t.lane_first_block = p;
+  p += nlanes;
+  t.lane_width = p;
+  p += nlanes;
+  t.lane_q_begin = p;
+  p += nlanes + 1;
+  t.queue = p;
+  t.counters = counters;
+  t.parts = parts;
+  t.err = err;
+  return t;
+}
+
+int plan_lanes(const std::vector<int>& widths, const std::vector<long long>& cells, int G,
+               LanePlan* out) {
+  const int nsys = (int)widths.size();
+  std::vector<int> cls = widths;
+  std::sort(cls.begin(), cls.end());
+  cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
+  long long need = 0;
+  for (int w : cls) need += w;
+  if (need > G) {
+    set_error_text("batch: lane widths of the distinct mesh sizes exceed the blocks available");
+    return EAF_EUNSUPPORTED;
+  }
+  const int C = (int)cls.size();
+  std::vector<std::vector<int>> members(C);
+  for (int s = 0; s < nsys; ++s)
+    members[std::lower_bound(cls.begin(), cls.end(), widths[s]) - cls.begin()].push_back(s);
+  std::vector<double> dur(nsys);
+  for (int s = 0; s < nsys; ++s) dur[s] = model_solve_us(cells[s], widths[s]);
+  for (auto& m : members)
+    std::sort(m.begin(), m.end(), [&](int x, int y) {
+      return dur[x] != dur[y] ? dur[x] > dur[y] : x < y;
+    });
+  auto lpt = [&](int c, int lanes, std::vector<std::vector<int>>* q) {
+    std::vector<double> load(lanes, 0.0);
+    if (q) q->assign(lanes, {});
+    for (int s : members[c]) {
+      int best = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[best] += dur[s];
+      if (q) (*q)[best].push_back(s);
+    }
+    return *std::max_element(load.begin(), load.end());
+  };
+  std::vector<int> lanes(C, 1);
+  int used = (int)need;
+  for (;;) {  // add a lane to the class that finishes last, while blocks remain
+    int worst = -1;
+    double worst_t = -1.0;
+    for (int c = 0; c < C; ++c) {
+      if ((int)members[c].size() <= lanes[c]) continue;  // one system per lane already
+      const double t = lpt(c, lanes[c], nullptr);
+      if (t > worst_t) { worst_t = t; worst = c; }
+    }
+    if (worst < 0 || used + cls[worst] > G) break;
+    lanes[worst] += 1;
+    used += cls[worst];
+  }
+  LanePlan& lp = *out;
+  lp.lane_of_block.assign(G, 0);
+  lp.lane_first.clear();
+  lp.lane_width.clear();
+  lp.q_begin.assign(1, 0);
+  lp.queue.clear();
+  int blk = 0;
+  for (int c = 0; c < C; ++c) {
+    std::vector<std::vector<int>> qs;
+    lpt(c, lanes[c], &qs);
+    for (auto& q : qs) {
+      const int L = (int)lp.lane_first.size();
+      lp.lane_first.push_back(blk);
+      lp.lane_width.push_back(cls[c]);
+      for (int k = 0; k < cls[c]; ++k) lp.lane_of_block[blk + k] = L;
+      blk += cls[c];
+      lp.queue.insert(lp.queue.end(), q.begin(), q.end());
+      lp.q_begin.push_back((int)lp.queue.size());
+    }
+  }
+  // leftover blocks: single-block lanes with empty queues
+  while (blk < G) {
+    const int L = (int)lp.lane_first.size();
+    lp.lane_first.push_back(blk);
+    lp.lane_width.push_back(1);
+    lp.lane_of_block[blk] = L;
+    lp.q_begin.push_back((int)lp.queue.size());
+    ++blk;
+  }
+  return EAF_OK;
+}
+
+}  // namespace eaf
 
 struct eaf_batch {
   int device, nsys;
@@ -140,112 +266,32 @@ int alloc_f32(eaf_batch* b) {
 // Lanes and queues (see the file comment).
 int plan(eaf_batch* b) {
   if (b->planned) return EAF_OK;
-  int per_sm64 = 0, per_sm32 = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm64, eaf::batch_f64_kernel_ptr(),
-                                                    kBatchBlock, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &per_sm32, eaf::batch_mixed_kernel_ptr(), kBatchBlock, 0) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device) !=
-          cudaSuccess) {
-    eaf::set_error("eaf_batch: occupancy query", cudaErrorUnknown);
-    return EAF_ECUDA;
-  }
-  const int G = std::min(std::min(per_sm64, per_sm32) * sms, eaf::kMaxGroupBlocks);
-  // classes of equal width
+  int G = 0;
+  int rc = eaf::batch_capacity(b->device, &G);
+  if (rc != EAF_OK) return rc;
   std::vector<int> widths;
   for (int s = 0; s < b->nsys; ++s) widths.push_back(width_for(b, s));
-  std::vector<int> cls = widths;
-  std::sort(cls.begin(), cls.end());
-  cls.erase(std::unique(cls.begin(), cls.end()), cls.end());
-  long long need = 0;
-  for (int w : cls) need += w;
-  if (need > G) {
-    eaf::set_error_text("eaf_batch: lane widths of the distinct mesh sizes exceed the "
-                        "co-resident blocks");
-    return EAF_EUNSUPPORTED;
-  }
-  const int C = (int)cls.size();
-  std::vector<std::vector<int>> members(C);
-  for (int s = 0; s < b->nsys; ++s)
-    members[std::lower_bound(cls.begin(), cls.end(), widths[s]) - cls.begin()].push_back(s);
-  std::vector<double> dur(b->nsys);
-  for (int s = 0; s < b->nsys; ++s) dur[s] = model_solve_us(b->n[s], widths[s]);
-  for (auto& m : members)
-    std::sort(m.begin(), m.end(), [&](int x, int y) {
-      return dur[x] != dur[y] ? dur[x] > dur[y] : x < y;
-    });
-  auto lpt = [&](int c, int lanes, std::vector<std::vector<int>>* out) {
-    std::vector<double> load(lanes, 0.0);
-    if (out) out->assign(lanes, {});
-    for (int s : members[c]) {
-      int best = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-      load[best] += dur[s];
-      if (out) (*out)[best].push_back(s);
-    }
-    return *std::max_element(load.begin(), load.end());
-  };
-  std::vector<int> lanes(C, 1);
-  int used = (int)need;
-  for (;;) {  // add a lane to the class that finishes last, while blocks remain
-    int worst = -1;
-    double worst_t = -1.0;
-    for (int c = 0; c < C; ++c) {
-      if ((int)members[c].size() <= lanes[c]) continue;  // one system per lane already
-      const double t = lpt(c, lanes[c], nullptr);
-      if (t > worst_t) { worst_t = t; worst = c; }
-    }
-    if (worst < 0 || used + cls[worst] > G) break;
-    lanes[worst] += 1;
-    used += cls[worst];
-  }
-  b->lane_of_block.assign(G, 0);
-  b->lane_first.clear();
-  b->lane_width.clear();
-  b->q_begin.assign(1, 0);
-  b->queue.clear();
-  int blk = 0;
-  for (int c = 0; c < C; ++c) {
-    std::vector<std::vector<int>> qs;
-    lpt(c, lanes[c], &qs);
-    for (auto& q : qs) {
-      const int L = (int)b->lane_first.size();
-      b->lane_first.push_back(blk);
-      b->lane_width.push_back(cls[c]);
-      for (int k = 0; k < cls[c]; ++k) b->lane_of_block[blk + k] = L;
-      blk += cls[c];
-      b->queue.insert(b->queue.end(), q.begin(), q.end());
-      b->q_begin.push_back((int)b->queue.size());
-    }
-  }
-  // leftover blocks: single-block lanes with empty queues
-  while (blk < G) {
-    const int L = (int)b->lane_first.size();
-    b->lane_first.push_back(blk);
-    b->lane_width.push_back(1);
-    b->lane_of_block[blk] = L;
-    b->q_begin.push_back((int)b->queue.size());
-    ++blk;
-  }
+  eaf::LanePlan lp;
+  rc = eaf::plan_lanes(widths, b->n, G, &lp);
+  if (rc != EAF_OK) return rc;
+  b->lane_of_block = lp.lane_of_block;
+  b->lane_first = lp.lane_first;
+  b->lane_width = lp.lane_width;
+  b->q_begin = lp.q_begin;
+  b->queue = lp.queue;
   b->grid = G;
   b->nlanes = (int)b->lane_first.size();
   // device tables
-  const size_t ntab = (size_t)G + 2 * b->nlanes + (b->nlanes + 1) + b->queue.size();
+  const std::vector<int> host = lp.packed();
   cudaFree(b->d_tab);
   cudaFree(b->d_counters);
   cudaFree(b->d_parts);
   b->d_tab = nullptr;
   b->d_counters = nullptr;
   b->d_parts = nullptr;
-  std::vector<int> host;
-  host.reserve(ntab);
-  host.insert(host.end(), b->lane_of_block.begin(), b->lane_of_block.end());
-  host.insert(host.end(), b->lane_first.begin(), b->lane_first.end());
-  host.insert(host.end(), b->lane_width.begin(), b->lane_width.end());
-  host.insert(host.end(), b->q_begin.begin(), b->q_begin.end());
-  host.insert(host.end(), b->queue.begin(), b->queue.end());
-  cudaError_t e = cudaMalloc((void**)&b->d_tab, sizeof(int) * ntab);
+  cudaError_t e = cudaMalloc((void**)&b->d_tab, sizeof(int) * host.size());
   if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_tab, host.data(), sizeof(int) * ntab, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(b->d_tab, host.data(), sizeof(int) * host.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMalloc((void**)&b->d_counters,
                    sizeof(unsigned long long) * eaf::kCounterStride * b->nlanes);
@@ -260,22 +306,8 @@ int plan(eaf_batch* b) {
 }
 
 BatchTables tables(const eaf_batch* b) {
-  BatchTables t;
-  const int* p = b->d_tab;
-  t.sys = b->d_sys;
-  t.lane_of_block = p;
-  p += b->grid;
-  t.lane_first_block = p;
-  p += b->nlanes;
-  t.lane_width = p;
-  p += b->nlanes;
-  t.lane_q_begin = p;
-  p += b->nlanes + 1;
-  t.queue = p;
-  t.counters = b->d_counters;
-  t.parts = b->d_parts;
-  t.err = b->d_err;
-  return t;
+  return eaf::tables_from(b->d_tab, b->grid, b->nlanes, b->d_sys, b->d_counters,
+                          b->d_parts, b->d_err);
 }
 
 // Everything one batched solve does on the device, in stream order.
@@ -292,10 +324,10 @@ cudaError_t enqueue(eaf_batch* b) {
   if (e == cudaSuccess) {
     const BatchTables t = tables(b);
     if (b->g_mixed)
-      e = eaf::launch_batch_mixed(t, b->grid, kBatchBlock, b->g_max_outer, b->g_max_iter,
+      e = eaf::launch_batch_mixed(t, b->grid, eaf::kBatchBlock, b->g_max_outer, b->g_max_iter,
                                   b->g_tol, b->g_inner_tol, b->timeout_ns, b->st);
     else
-      e = eaf::launch_batch_f64(t, b->grid, kBatchBlock, b->g_max_iter, b->g_tol,
+      e = eaf::launch_batch_f64(t, b->grid, eaf::kBatchBlock, b->g_max_iter, b->g_tol,
                                 b->timeout_ns, b->st);
   }
   if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->ev1, b->st, cudaEventRecordExternal);
@@ -429,7 +461,7 @@ int eaf_batch_plan(eaf_batch_t b, int* grid, int* block, int* nlanes) {
   const int rc = plan(b);
   if (rc != EAF_OK) return rc;
   *grid = b->grid;
-  *block = kBatchBlock;
+  *block = eaf::kBatchBlock;
   *nlanes = b->nlanes;
   return EAF_OK;
 }

@@ -195,6 +195,58 @@ int eaf_batch_get_phi(eaf_batch_t b, int sys, double* phi);
 double eaf_batch_last_ms(eaf_batch_t b);
 void* eaf_batch_stream(eaf_batch_t b);
 
+/* ---- serving loop --------------------------------------------------------- */
+/* No reference counterpart. A host-side request loop for concurrent
+ * simulated furnace runs: each run's state (coefficients, Krylov workspace,
+ * and phi as the warm start) stays on the device between its solves; runs
+ * are admitted against an HBM budget; requests are solved in batched
+ * persistent launches (continuous batching: new requests go out in the next
+ * batch as soon as a stream slot and blocks are free; two batches may be in
+ * flight). A run's result does not depend on which other runs share its
+ * batches. Thread-safe; a submitted request reads the caller's input arrays
+ * until its ticket completes and writes phi_out (if not NULL) before. */
+typedef struct eaf_srv* eaf_srv_t;
+typedef struct {
+  long long solves, batches, admitted_runs, refused_runs, active_runs;
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> completion latency */
+  double solves_per_s;                     /* first submit to last completion */
+  double mean_batch, used_bytes, budget_bytes;
+} eaf_srv_stats_t;
+enum { EAF_FAULT_DEVICE_LOST = 1 };
+
+/* mixed = 0: plain FP64 (max_iter, tol as eaf_cg_solve_f64); mixed = 1:
+ * max_iter inner iterations per refinement step, max_outer steps,
+ * inner_tol (as eaf_cg_solve_mixed). max_batch bounds requests per batch. */
+int eaf_srv_create(eaf_srv_t* out, int device, double hbm_budget_bytes,
+                   int mixed, int max_iter, double tol, int max_outer,
+                   double inner_tol, int max_batch);
+/* Finishes every queued and in-flight request, then frees everything. */
+int eaf_srv_destroy(eaf_srv_t s);
+/* Admission: EAF_EADMIT if the run's device state would exceed the budget.
+ * The run's warm start starts at zero. */
+int eaf_srv_open_run(eaf_srv_t s, int nr, int nth, int nz, int* run_id);
+/* EAF_EBUSY while the run has a request outstanding. */
+int eaf_srv_close_run(eaf_srv_t s, int run_id);
+/* One pressure solve for the run (reference halo-layout host arrays; phi_out
+ * receives the solution in the same layout). EAF_EBUSY if the run already
+ * has a request outstanding (SIMPLE is sequential per run). */
+int eaf_srv_submit(eaf_srv_t s, int run_id, const double* aW, const double* aE,
+                   const double* aS, const double* aN, const double* aB,
+                   const double* aT, const double* aP, const double* Su,
+                   double* phi_out, long long* ticket);
+/* EAF_EBUSY until the request is done; then its result (once). */
+int eaf_srv_poll(eaf_srv_t s, long long ticket, double* residual, int* n_iter,
+                 int* n_outer, int* status);
+/* Waits at most timeout_ms (EAF_ETIMEOUT otherwise). */
+int eaf_srv_wait(eaf_srv_t s, long long ticket, double timeout_ms,
+                 double* residual, int* n_iter, int* n_outer, int* status);
+int eaf_srv_stats(eaf_srv_t s, eaf_srv_stats_t* st);
+int eaf_srv_reset_stats(eaf_srv_t s);
+/* Failure-detection hook: simulates the loss of the device in the server's
+ * host logic (no GPU fault): queued and in-flight requests complete with
+ * EAF_ECUDA and new work is refused with EAF_ECLOSED. */
+int eaf_srv_inject_fault(eaf_srv_t s, int kind);
+
 /* ---- no-allocation entry point ----------------------------------------- */
 /* No counterpart in the reference. For callers that must not allocate
  * device memory: a simulator whose device memory is owned by its own pool
