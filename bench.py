@@ -67,7 +67,7 @@ def measured_peaks():
 def ncu_traffic_per_cell_iter():
     """DRAM bytes per cell-iteration of the solver kernel from the committed
     ncu summary, or None when no capture has been summarised yet."""
-    path = os.path.join(ROOT, "profiles", "cg_f64_production_ncu.txt")
+    path = os.path.join(ROOT, "profiles", "cg_f64_kernel_60x120x84.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -344,6 +344,197 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Further named workloads (one JSON line each; not the driver's headline)
+# ---------------------------------------------------------------------------
+def _base_line(metric, value, unit, steps, warmup, ms_per_step, workload, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": DATA, "config": {"workload": workload}}
+    line["config"].update(extra)
+    return line
+
+
+def run_fine(args):
+    """120x240x168, 64 spheres: FP64 plain solves (HBM-bound roofline case)
+    and the mixed FP32/FP64 form on the same system, with its error against
+    the FP64 solution."""
+    import numpy as np
+    import torch
+    eaf = importlib.import_module(PKG)
+    g = importlib.import_module(PKG + ".eafgen")
+    nr, nth, nz, nsph = g.FINE
+    n = nr * nth * nz
+    s = g.make_system(nr, nth, nz, nsph, seed=0)
+    dev = [torch.from_numpy(a).cuda() for a in s.arrays()]
+    phi = torch.zeros(g.halo_shape(nr, nth, nz), dtype=torch.float64, device="cuda")
+    with eaf.CGSolver(nr, nth, nz) as cg:
+        for _ in range(args.warmup):           # warm-ups capped at 300 iterations
+            phi.zero_()
+            cg.solve(dev, phi, 300, 0.0, device_ptrs=True)
+        ms, kms, its = 0.0, 0.0, []
+        for _ in range(args.steps):
+            phi.zero_()
+            torch.cuda.synchronize()
+            res, nit, st = cg.solve(dev, phi, MAX_ITER, 1e-10, device_ptrs=True)
+            t = cg.last_timing()
+            ms += t["solve_ms"]
+            kms += t["kernel_ms"]
+            its.append(nit)
+        x64 = phi.cpu().numpy()
+        launch = cg.last_launch()
+        phim = torch.zeros_like(phi)
+        rm, nm, no, stm = cg.solve_mixed(dev, phim, tol=1e-10, inner_tol=0.1,
+                                         max_outer=args.mixed_outer,
+                                         max_inner=args.mixed_inner, device_ptrs=True)
+        tm = cg.last_timing()
+        xm = phim.cpu().numpy()
+    I = g.interior
+    err = float(np.linalg.norm(I(xm) - I(x64)) / np.linalg.norm(I(x64)))
+    ci = n * sum(its)
+    value = ci / (ms / 1e3)
+    achieved = BYTES_PER_CELL_ITER * ci / (kms / 1e3) / 1e9
+    peak, kind = measured_peaks()
+    line = _base_line("pressure-CG cell-iters/s (120x240x168, FP64, tol 1e-10)", value,
+                      "cell-iters/s", args.steps, args.warmup, ms / args.steps,
+                      "pressure-CG 120x240x168 FP64 cold solves",
+                      {"mesh": [nr, nth, nz], "cells": n, "tol": 1e-10,
+                       "iterations_per_solve": its,
+                       "launch": {"grid": launch[0], "block": launch[1]}})
+    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": f"{kind} hbm_gbs",
+                        "kernel": "cg_f64_kernel"}
+    line["mixed"] = {"residual": rm, "status": stm, "inner_iterations": nm,
+                     "outer_steps": no, "kernel_ms": tm["kernel_ms"],
+                     "caps": {"max_outer": args.mixed_outer, "max_inner": args.mixed_inner},
+                     "rel_l2_error_vs_fp64": err,
+                     "fp64_kernel_ms_per_solve": kms / args.steps}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args):
+    """96 uneven systems (40 at 12x24x16, 30 at 18x36x24, 20 at 35x70x50,
+    6 at 60x120x84; seed = system id) in one persistent launch replayed from
+    a CUDA graph, against the same systems solved one by one."""
+    import torch
+    eaf = importlib.import_module(PKG)
+    g = importlib.import_module(PKG + ".eafgen")
+    systems = []
+    for (dims, count) in g.BATCH_MIX:
+        for _ in range(count):
+            systems.append(g.make_system(*dims, seed=len(systems)))
+    dims = [(s.nr, s.nth, s.nz) for s in systems]
+    dev = [[torch.from_numpy(a).cuda() for a in s.arrays()] for s in systems]
+    phis = [torch.zeros(g.halo_shape(*d), dtype=torch.float64, device="cuda") for d in dims]
+    total_cells = sum(a * b * c for a, b, c in dims)
+    out = {}
+    with eaf.Batch(dims) as b:
+        for i in range(len(systems)):
+            b.set_system(i, dev[i][:8], phis[i], device_ptrs=True)
+        grid, block, nlanes = b.plan()
+        for form in ("fp64", "mixed"):
+            mixed = form == "mixed"
+            kw = dict(mixed=mixed, max_iter=args.mixed_inner if mixed else MAX_ITER,
+                      tol=TOL, max_outer=args.mixed_outer, inner_tol=0.1)
+            for _ in range(args.warmup if not mixed else 1):
+                for p in phis:
+                    p.zero_()
+                b.solve(**kw)
+            ms, ci, worst = 0.0, 0, 0.0
+            steps = args.steps if not mixed else 1
+            for _ in range(steps):
+                for p in phis:
+                    p.zero_()
+                torch.cuda.synchronize()
+                b.solve(**kw)
+                ms += b.last_ms
+                for i in range(len(systems)):
+                    r, nit, no, st = b.result(i)
+                    ci += (dims[i][0] * dims[i][1] * dims[i][2]) * nit
+                    worst = max(worst, r)
+            out[form] = {"ms_per_batch": ms / steps, "cell_iters_per_s": ci / (ms / 1e3),
+                         "solves_per_s": len(systems) * steps / (ms / 1e3),
+                         "max_residual": worst}
+        widths = sorted({(d, b.lane_width(i)) for i, d in enumerate(dims)})
+    # the same systems one by one through the single-system FP64 solver
+    seq_ms = 0.0
+    for i, s in enumerate(systems):
+        with eaf.CGSolver(*dims[i]) as cg:
+            phis[i].zero_()
+            cg.solve(dev[i][:8], phis[i], MAX_ITER, TOL, device_ptrs=True)
+            phis[i].zero_()
+            torch.cuda.synchronize()
+            cg.solve(dev[i][:8], phis[i], MAX_ITER, TOL, device_ptrs=True)
+            seq_ms += cg.last_timing()["solve_ms"]
+    seq = {"ms_per_96": seq_ms, "solves_per_s": len(systems) / (seq_ms / 1e3)}
+    line = _base_line("batched pressure-CG solves/s (96-system mix, one launch)",
+                      out["fp64"]["solves_per_s"], "solves/s", args.steps, args.warmup,
+                      out["fp64"]["ms_per_batch"], "96 uneven systems, one persistent launch",
+                      {"systems": len(systems), "cells": total_cells,
+                       "mix": [[list(d[:3]), c] for d, c in g.BATCH_MIX],
+                       "plan": {"grid": grid, "block": block, "lanes": nlanes},
+                       "lane_widths": [[list(d), w] for d, w in widths],
+                       "graph": "pack + persistent batch kernel + unpack captured once, replayed"})
+    line["forms"] = out
+    line["sequential_fp64"] = seq
+    line["speedup_vs_sequential_fp64"] = out["fp64"]["solves_per_s"] / seq["solves_per_s"]
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """Poisson arrivals of simulated furnace runs (serving mix), 50 warm-
+    started solves per run, continuous batching; p50/p99 per rate."""
+    eaf = importlib.import_module(PKG)
+    g = importlib.import_module(PKG + ".eafgen")
+    sc = importlib.import_module(PKG + ".serve_client")
+    mix = g.SERVE_MIX
+    pool = sc.build_pool(g, eaf, mix, 4, 0)
+    rates = [float(r) for r in args.rates.split(",")]
+    points = []
+    for mixed in ([False, True] if args.serve_mixed else [False]):
+        with eaf.Server(budget_bytes=150e9, mixed=mixed,
+                        max_iter=args.mixed_inner if mixed else MAX_ITER, tol=TOL,
+                        max_outer=args.mixed_outer, inner_tol=0.1) as srv:
+            for rate in (rates if not mixed else rates[:1]):
+                st = sc.run_stream(srv, g, eaf, pool, mix, rate,
+                                   duration=args.serve_runs / rate, solves=args.solves_per_run,
+                                   seed=int(rate * 100), max_wall=900.0)
+                st.update({"rate_runs_per_s": rate, "mixed": mixed})
+                points.append(st)
+    # plain FP64 per-solve path on the same pool, one solve at a time
+    import numpy as np
+    per = {}
+    for (dims, share) in mix:
+        nr, nth, nz, _ = dims
+        with eaf.CGSolver(nr, nth, nz) as cg:
+            phi = eaf.host_empty(g.halo_shape(nr, nth, nz))
+            phi[...] = 0.0
+            times = []
+            for k, arrs in enumerate(pool[dims]):
+                cg.solve(arrs, phi, MAX_ITER, TOL)
+                times.append(cg.last_timing()["e2e_ms"])
+            per[str([nr, nth, nz])] = float(np.mean(times[1:] if len(times) > 1 else times))
+    mean_ms = sum(share * per[str(list(d[:3]))] for d, share in mix)
+    first = [p for p in points if not p["mixed"]]
+    best = max(first, key=lambda p: p["solves_per_s"])
+    line = _base_line("serve p99 latency @1e-8 resid (Poisson furnace runs)",
+                      best["p99_ms"], "ms", len(points), 0, best["mean_ms"],
+                      "serving stream, continuous batching",
+                      {"mix": [[list(d[:3]), sh] for d, sh in mix],
+                       "solves_per_run": args.solves_per_run,
+                       "runs_per_rate": args.serve_runs,
+                       "rates_runs_per_s": rates, "budget_gb": 150})
+    line["higher_is_better"] = False
+    line["points"] = points
+    line["per_solve_fp64"] = {"mean_ms_by_mesh": per, "mix_mean_ms": mean_ms,
+                              "solves_per_s": 1e3 / mean_ms}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,7 +543,17 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-iters", type=int, default=1500,
                     help="iteration cap per reference-arm step (bounded sample)")
+    ap.add_argument("--workload", choices=["production", "fine", "batch", "serve"],
+                    default="production")
+    ap.add_argument("--mixed-outer", type=int, default=30)
+    ap.add_argument("--mixed-inner", type=int, default=3000)
+    ap.add_argument("--rates", default="5,20,50,200")
+    ap.add_argument("--serve-runs", type=int, default=25)
+    ap.add_argument("--solves-per-run", type=int, default=50)
+    ap.add_argument("--serve-mixed", action="store_true")
     args = ap.parse_args(argv)
+    if args.workload != "production" and args.impl == "ours":
+        return {"fine": run_fine, "batch": run_batch, "serve": run_serve}[args.workload](args)
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local_rank = _env_int("LOCAL_RANK", 0)

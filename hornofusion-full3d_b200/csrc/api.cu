@@ -11,6 +11,7 @@
 #include "cg_kernels.h"
 #include "eafcg.h"
 #include "eafcg_internal.h"
+#include "tune_table.h"
 
 using eaf::GroupWs;
 using eaf::HaloInputs;
@@ -108,12 +109,21 @@ static int max_coresident(const void* kernel, int block, int sms) {
   return per_sm * sms;
 }
 
-// Launch shape for a persistent kernel over n cells.
+// Launch shape for a persistent kernel over n cells: an explicit
+// eaf_cg_set_launch shape, else the tuned shape of this mesh (FP64 solver),
+// else one 1024-thread block up to 8192 cells or one 512-thread block per
+// 2048 cells; capped by co-residency.
 static void pick_launch(const eaf_cg* h, const void* kernel, int* grid, int* block) {
   int b = h->block > 0 ? h->block : kDefaultBlock;
   int cap = max_coresident(kernel, b, h->sms);
   int g;
-  if (h->grid > 0) {
+  int tb = 0, tg = 0;
+  if (h->block == 0 && h->grid == 0 && kernel == eaf::cg_f64_kernel_ptr() &&
+      eaf::tuned_single_launch(h->nr, h->nth, h->nz, &tb, &tg)) {
+    b = tb;
+    cap = max_coresident(kernel, b, h->sms);
+    g = tg;
+  } else if (h->grid > 0) {
     g = h->grid;
   } else if (h->d.n <= 8192) {
     b = h->block > 0 ? h->block : 1024;

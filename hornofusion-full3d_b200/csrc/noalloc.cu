@@ -35,6 +35,7 @@
 #include "cg_kernels.h"
 #include "eafcg.h"
 #include "eafcg_internal.h"
+#include "tune_table.h"
 
 namespace {
 
@@ -146,12 +147,14 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
   ws.err = reinterpret_cast<int*>(base + kErrOff);
   ws.result = reinterpret_cast<eaf::SolveResult*>(base + kResultOff);
 
-  // Launch shape: the default of eaf_cg_create handles (one 1024-thread
-  // block up to 8192 cells, else one 512-thread block per 2048 cells),
-  // capped by co-residency, so that results match the handle entry points
-  // bit for bit.
+  // Launch shape: the default of eaf_cg_create handles (the tuned shape of
+  // the mesh; else one 1024-thread block up to 8192 cells or one 512-thread
+  // block per 2048 cells), capped by co-residency, so that results match the
+  // handle entry points bit for bit.
   int block = 512, grid;
-  if (n <= 8192) {
+  if (eaf::tuned_single_launch(nr, nth, nz, &block, &grid)) {
+    // the tuned shape of this mesh, as the handle entry points use
+  } else if (n <= 8192) {
     block = 1024;
     grid = 1;
   } else {

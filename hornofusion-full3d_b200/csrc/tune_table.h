@@ -1,6 +1,6 @@
-// Lane width (blocks of 512 threads) per mesh for batched and served solves.
-// Generated by hornofusion-full3d_b200/autotune.py; the fallback rule below
-// covers meshes that are not in the table.
+// Launch shapes measured on B200 by hornofusion-full3d_b200/autotune.py
+// (tune_table.json beside it holds every measurement). Meshes that are not
+// in a table fall back to the rules below.
 #pragma once
 
 namespace eaf {
@@ -9,11 +9,12 @@ struct TunedWidth {
   int nr, nth, nz, width;
 };
 
+// Lane width (blocks of 512 threads) of batched and served solves.
 static const TunedWidth kTunedWidths[] = {
     {12, 24, 16, 1},
-    {18, 36, 24, 1},
-    {35, 70, 50, 8},
-    {60, 120, 84, 37},
+    {18, 36, 24, 4},
+    {35, 70, 50, 32},
+    {60, 120, 84, 48},
 };
 
 inline int tuned_lane_width(int nr, int nth, int nz) {
@@ -22,6 +23,29 @@ inline int tuned_lane_width(int nr, int nth, int nz) {
   const long long n = (long long)nr * nth * nz;
   long long w = (n + 16383) / 16384;  // about 32 cells per thread
   return (int)(w < 1 ? 1 : (w > 64 ? 64 : w));
+}
+
+struct TunedLaunch {
+  int nr, nth, nz, block, grid;
+};
+
+// (block, grid) of the single-system persistent solver.
+static const TunedLaunch kTunedLaunches[] = {
+    {12, 24, 16, 256, 18},
+    {18, 36, 24, 256, 32},
+    {35, 70, 50, 512, 148},
+    {60, 120, 84, 1024, 148},
+    {120, 240, 168, 1024, 148},
+};
+
+inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid) {
+  for (const TunedLaunch& t : kTunedLaunches)
+    if (t.nr == nr && t.nth == nth && t.nz == nz) {
+      *block = t.block;
+      *grid = t.grid;
+      return true;
+    }
+  return false;
 }
 
 }  // namespace eaf

@@ -1,0 +1,99 @@
+"""Multi-GPU host logic: independent systems sharded across ranks.
+
+One pressure system never spans GPUs (the whole theta x z domain stays on
+one device), so there is no data-path collective: batches of systems and
+serving streams are partitioned across ranks by footprint and estimated
+work, each rank solves its share on its own GPU, and only timings and small
+per-system results travel, on the host side, through torch.distributed
+(NCCL on GPU ranks, gloo for CPU-side checks).
+
+The reference's own parallelism -- MPI domain decomposition with two-layer
+halos and scalar allreduces (src/mod_mpi_topology.f90:79-285,291-417) -- is
+not used: it would split a single system, which this design never does.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+
+@dataclass(frozen=True)
+class Item:
+    """One independent system or run to place."""
+    key: int
+    cells: int
+    footprint: float   # device bytes
+    work: float        # estimated cost (any unit, e.g. cell-iterations)
+
+
+def estimated_work(nr: int, nth: int, nz: int) -> float:
+    """Cell-iterations of a solve to 1e-8 on these meshes (iterations grow
+    about as 8 sqrt(cells) for the synthetic furnace operators)."""
+    n = nr * nth * nz
+    return n * 8.0 * math.sqrt(n)
+
+
+def device_footprint(nr: int, nth: int, nz: int, mixed: bool = False) -> float:
+    """Device bytes of one resident system (compact FP64 state, halo-layout
+    staging, FP32 shadow when mixed) -- the server's admission figure."""
+    n = nr * nth * nz
+    nh = (nr + 4) * (nth + 4) * (nz + 4)
+    b = n * 8 * 14 + nh * 8 * 9 + 256
+    if mixed:
+        b += n * 4 * 13
+    return float(b)
+
+
+def partition(items: list[Item], n_ranks: int,
+              budget: float | None = None) -> list[list[Item]]:
+    """Longest-processing-time assignment: items by decreasing work, each to
+    the rank with the least assigned work that still has room in its device
+    budget. Deterministic (ties go to the lower rank). Raises if an item
+    fits on no rank."""
+    if n_ranks < 1:
+        raise ValueError("n_ranks must be >= 1")
+    load = [0.0] * n_ranks
+    used = [0.0] * n_ranks
+    out: list[list[Item]] = [[] for _ in range(n_ranks)]
+    for it in sorted(items, key=lambda i: (-i.work, i.key)):
+        order = sorted(range(n_ranks), key=lambda r: (load[r], r))
+        for r in order:
+            if budget is None or used[r] + it.footprint <= budget:
+                out[r].append(it)
+                load[r] += it.work
+                used[r] += it.footprint
+                break
+        else:
+            raise RuntimeError(f"item {it.key} ({it.footprint:.3g} B) fits on no rank")
+    return out
+
+
+def reduce_timing(elapsed_s: float, units: float, group=None) -> tuple[float, float]:
+    """(max elapsed over ranks, total units over ranks): the whole-job time is
+    the slowest rank's, the work is everybody's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return elapsed_s, units
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor([elapsed_s], dtype=torch.float64, device=dev)
+    u = torch.tensor([units], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM, group=group)
+    return float(t.item()), float(u.item())
+
+
+def gather_results(local: dict, group=None) -> dict:
+    """Per-key results of every rank, merged on every rank."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return dict(local)
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, local, group=group)
+    merged = {}
+    for p in parts:
+        overlap = set(merged) & set(p)
+        if overlap:
+            raise RuntimeError(f"keys solved on two ranks: {sorted(overlap)[:5]}")
+        merged.update(p)
+    return merged
