@@ -9,8 +9,9 @@
 // admits runs against an HBM budget, and solves their requests in batched
 // persistent launches (batch.cu kernels):
 //
-//   * continuous batching: requests that arrive while batches are on the
-//     GPU wait in a FIFO and go out in the next batch as soon as a stream
+//   * continuous batching, by size: requests that arrive while batches are
+//     on the GPU wait in a FIFO; the next batch takes the oldest request's
+//     mesh size and the queued requests of that size, as soon as a stream
 //     slot and enough blocks are free; up to two batches are in flight on
 //     separate streams, so uploads, downloads and compute of different
 //     batches overlap;
@@ -206,26 +207,31 @@ bool launch(eaf_srv* s, std::unique_lock<std::mutex>& lk) {
     if (!c.busy) { sl = &c; break; }
   if (!sl) return false;
   const int free_blocks = s->capacity - s->blocks_in_use;
-  // FIFO selection while the lane widths of the selected mesh sizes fit.
+  // Batches by size: the oldest pending request fixes the batch's mesh (lane
+  // width class); requests of that mesh join in FIFO order while their
+  // lanes fit. A batch's persistent launch ends when its slowest solve
+  // does, so a batch of one mesh size keeps short solves from waiting on
+  // long ones; the second stream slot runs another size meanwhile.
   std::vector<Pick> pick;
   std::vector<int> widths;
   std::vector<long long> cells;
-  std::vector<int> classes;
-  int class_sum = 0;
+  int used = 0, cls_nr = -1, cls_nth = -1, cls_nz = -1;
   for (auto it = s->pending.begin(); it != s->pending.end();) {
     if ((int)pick.size() >= s->max_batch) break;
     const SrvTicket& t = s->tickets[*it];
     SrvRun* r = s->runs[t.run];
-    const int w = eaf::tuned_lane_width(r->nr, r->nth, r->nz);
-    const bool new_class = std::find(classes.begin(), classes.end(), w) == classes.end();
-    if (new_class && class_sum + w > free_blocks) {
+    if (cls_nr < 0) {
+      cls_nr = r->nr;
+      cls_nth = r->nth;
+      cls_nz = r->nz;
+    }
+    if (r->nr != cls_nr || r->nth != cls_nth || r->nz != cls_nz) {
       ++it;
       continue;
     }
-    if (new_class) {
-      classes.push_back(w);
-      class_sum += w;
-    }
+    const int w = eaf::tuned_lane_width(r->nr, r->nth, r->nz);
+    if (used + w > free_blocks) break;
+    used += w;
     Pick p;
     p.id = *it;
     p.run = r;

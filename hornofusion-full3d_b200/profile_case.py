@@ -25,7 +25,12 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--launch", type=int, nargs=2, default=None)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="solve this many copies of the mixed batch instead "
+                         "(12x24x16, 18x36x24, 35x70x50, 60x120x84 round robin)")
     args = ap.parse_args(argv)
+    if args.batch:
+        return batch_case(args)
     import torch
     eaf = importlib.import_module("hornofusion-full3d_b200")
     g = importlib.import_module("hornofusion-full3d_b200.eafgen")
@@ -54,6 +59,32 @@ def main(argv=None):
                         "us_per_iter": 1e3 * t["kernel_ms"] / max(nit, 1)})
     print(json.dumps({"mesh": [nr, nth, nz], "launch": [grid, block],
                       "mixed": args.mixed, "runs": out}))
+    return 0
+
+
+def batch_case(args):
+    import torch
+    eaf = importlib.import_module("hornofusion-full3d_b200")
+    g = importlib.import_module("hornofusion-full3d_b200.eafgen")
+    meshes = [d for d, _ in g.BATCH_MIX]
+    systems = [g.make_system(*meshes[k % len(meshes)], seed=k) for k in range(args.batch)]
+    dims = [(s.nr, s.nth, s.nz) for s in systems]
+    dev = [[torch.from_numpy(a).cuda() for a in s.arrays()] for s in systems]
+    phis = [torch.zeros(g.halo_shape(*d), dtype=torch.float64, device="cuda") for d in dims]
+    out = []
+    with eaf.Batch(dims) as b:
+        for i in range(len(systems)):
+            b.set_system(i, dev[i], phis[i], device_ptrs=True)
+        for _ in range(args.repeat):
+            for p in phis:
+                p.zero_()
+            torch.cuda.synchronize()
+            b.solve(max_iter=args.iters, tol=0.0)
+            cells = sum(d[0] * d[1] * d[2] for d in dims)
+            out.append({"batch_ms": b.last_ms,
+                        "cell_iters_per_s": cells * args.iters / (b.last_ms / 1e3)})
+        plan = b.plan()
+    print(json.dumps({"batch": dims, "plan": plan, "runs": out}))
     return 0
 
 
