@@ -112,27 +112,29 @@ static int max_coresident(const void* kernel, int block, int sms) {
 // Launch shape for a persistent kernel over n cells: an explicit
 // eaf_cg_set_launch shape, else the tuned shape of this mesh (FP64 solver),
 // else one 1024-thread block up to 8192 cells or one 512-thread block per
-// 2048 cells; capped by co-residency.
-static void pick_launch(const eaf_cg* h, const void* kernel, int* grid, int* block) {
+// 2048 cells; capped by co-residency of the kernel (variant) that runs
+// blocks of that size.
+static void pick_launch(const eaf_cg* h, bool f64, int* grid, int* block) {
+  auto kernel_for = [f64](int b) {
+    return f64 ? eaf::cg_f64_kernel_ptr(b) : eaf::cg_mixed_kernel_ptr();
+  };
   int b = h->block > 0 ? h->block : kDefaultBlock;
-  int cap = max_coresident(kernel, b, h->sms);
   int g;
   int tb = 0, tg = 0;
-  if (h->block == 0 && h->grid == 0 && kernel == eaf::cg_f64_kernel_ptr() &&
+  if (h->block == 0 && h->grid == 0 && f64 &&
       eaf::tuned_single_launch(h->nr, h->nth, h->nz, &tb, &tg)) {
     b = tb;
-    cap = max_coresident(kernel, b, h->sms);
     g = tg;
   } else if (h->grid > 0) {
     g = h->grid;
   } else if (h->d.n <= 8192) {
     b = h->block > 0 ? h->block : 1024;
-    cap = max_coresident(kernel, b, h->sms);
     g = 1;
   } else {
     long long want = ((long long)h->d.n + (long long)b * 4 - 1) / ((long long)b * 4);
     g = (int)(want < 1 ? 1 : want);
   }
+  const int cap = max_coresident(kernel_for(b), b, h->sms);
   if (cap > 0 && g > cap) g = cap;
   if (g > h->sms * 8) g = h->sms * 8;
   *grid = g;
@@ -245,7 +247,7 @@ int eaf_cg_set_launch(eaf_cg_t h, int block_threads, int grid_blocks) {
 int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks) {
   if (!h || !block_threads || !grid_blocks) return EAF_EINVAL;
   eaf::DeviceGuard guard(h->device);
-  pick_launch(h, eaf::cg_f64_kernel_ptr(), grid_blocks, block_threads);
+  pick_launch(h, true, grid_blocks, block_threads);
   return EAF_OK;
 }
 
@@ -346,13 +348,13 @@ int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts&
   if (o.mixed) {
     int rc = ensure_f32(h);
     if (rc != EAF_OK) return rc;
-    pick_launch(h, eaf::cg_mixed_kernel_ptr(), &grid, &block);
+    pick_launch(h, false, &grid, &block);
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     EAF_CUDA(eaf::launch_cg_mixed(h->d, h->s, h->f, h->ws, o.max_outer, o.max_iter,
                                   o.tol, o.inner_tol, h->timeout_ns, grid, block,
                                   h->st));
   } else {
-    pick_launch(h, eaf::cg_f64_kernel_ptr(), &grid, &block);
+    pick_launch(h, true, &grid, &block);
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     EAF_CUDA(eaf::launch_cg_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
                                 grid, block, h->st));

@@ -114,6 +114,12 @@ __device__ __forceinline__ void fence_acq_rel_gpu() {
 //      the acquire that observes the last arrival orders what follows);
 //   2  release add, relaxed polls, one acquire fence after the last poll.
 constexpr int kBarrierForm = 1;
+// Form of group_allsum: 0-2 as above (full block barriers around the group
+// barrier), 3 the warp-0 form with split block barriers (group_allsum_w0).
+#ifndef EAF_ALLSUM_FORM
+#define EAF_ALLSUM_FORM 3
+#endif
+constexpr int kAllsumForm = EAF_ALLSUM_FORM;
 
 template <int FORM = kBarrierForm>
 __device__ __forceinline__ bool group_barrier(Group& g) {
@@ -193,12 +199,128 @@ static __device__ __forceinline__ double* group_stage_smem() {
   return s_stage;
 }
 
+// ---------------------------------------------------------------------------
+// Warp-0 group all-reduce with split block barriers. Same association as
+// group_allsum (so bit-identical totals) with fewer block-wide waits: the
+// other warps post their warp sums and arrive (bar.arrive, no wait) on named
+// barrier kBarPosted; warp 0 waits there, folds the block partial, publishes
+// it with a release add on the group counter, polls the counter (every lane
+// acquires), loads the nb block partials straight into registers, folds them
+// and arrives on kBarTotal, where the other warps wait for the totals. Each
+// block-wide phase is one arrive/wait pair instead of four full barriers.
+// Named barriers 1 and 2 are reserved for it; the reuse order is safe because
+// a warp arrives on one barrier only after passing the other.
+// ---------------------------------------------------------------------------
+constexpr int kBarPosted = 1;
+constexpr int kBarTotal = 2;
+
+__device__ __forceinline__ void named_arrive(int id, int nthreads) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ void named_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+template <int NV, typename T>
+__device__ __forceinline__ bool group_allsum_w0(T (&v)[NV], Group& g, int slot) {
+  __shared__ T s_w[NV][32];
+  __shared__ double s_tot[NV];
+  __shared__ int s_ok;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nthreads = blockDim.x;
+#pragma unroll
+  for (int m = 0; m < NV; ++m) v[m] = warp_allsum(v[m]);
+  if (w != 0) {
+    if (lane == 0) {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) s_w[m][w] = v[m];
+    }
+    named_arrive(kBarPosted, nthreads);
+    named_sync(kBarTotal, nthreads);
+#pragma unroll
+    for (int m = 0; m < NV; ++m) v[m] = (T)s_tot[m];
+    return s_ok != 0;
+  }
+  // Warp 0.
+  if (lane == 0) {
+#pragma unroll
+    for (int m = 0; m < NV; ++m) s_w[m][0] = v[m];
+  }
+  named_sync(kBarPosted, nthreads);
+  const int nw = (nthreads + 31) >> 5;
+  double blk[NV];
+#pragma unroll
+  for (int m = 0; m < NV; ++m) blk[m] = (double)warp_allsum(lane < nw ? s_w[m][lane] : T(0));
+  int ok = 1;
+  if (g.nb == 1) {
+    if (lane == 0) {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) s_tot[m] = blk[m];
+    }
+  } else {
+    // Thread 0's count is authoritative (group_barrier advances only it).
+    g.epoch = __shfl_sync(0xffffffffu, g.epoch, 0) + 1;
+    const unsigned long long target = g.epoch * (unsigned long long)g.nb;
+    if (lane == 0) {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) g.part[(size_t)(slot + m) * g.nb + g.bid] = blk[m];
+      red_release_add_u64(g.counter, 1ull);
+    }
+    if (lane == 0) {
+      uint64_t t0 = 0;
+      uint32_t spins = 0;
+      while (ld_acquire_u64(g.counter) < target) {
+        if ((++spins & 63u) == 0) {
+          if (spins == 64u) t0 = global_ns();
+          if (ld_volatile_i32(g.err) != 0) { ok = 0; break; }
+          if (global_ns() - t0 > g.timeout_ns) {
+            atomicCAS(g.err, 0, (int)EAF_ETIMEOUT);
+            ok = 0;
+            break;
+          }
+        }
+      }
+    }
+    // bar.warp.sync orders the other lanes' loads after lane 0's acquire.
+    __syncwarp();
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    // All of this lane's partials in one round of independent loads (groups
+    // of up to kMaxGroupBlocks / 32 = 37 per sum), then the fixed-order fold.
+    constexpr int kPer = 8;
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      const double* p = g.part + (size_t)(slot + m) * g.nb;
+      double sum = 0.0;
+      for (int b0 = lane; b0 < g.nb; b0 += 32 * kPer) {
+        double t[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+          const int b = b0 + 32 * u;
+          t[u] = b < g.nb ? __ldcg(p + b) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u)
+          if (b0 + 32 * u < g.nb) sum = sum + t[u];
+      }
+      sum = warp_allsum(sum);
+      if (lane == 0) s_tot[m] = sum;
+    }
+  }
+  if (lane == 0) s_ok = ok;
+  named_arrive(kBarTotal, nthreads);
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < NV; ++m) v[m] = (T)s_tot[m];
+  return ok != 0;
+}
+
 // Group all-reduce of NV sums. Per-thread and in-block sums are carried in
 // T (FP32 for the mixed-precision inner solve, FP64 otherwise); block
 // partials go to slots [slot, slot+NV) of the group's FP64 partial table and
 // are folded in FP64. Returns false if the barrier gave up.
-template <int NV, typename T, int FORM = kBarrierForm>
+template <int NV, typename T, int FORM = kAllsumForm>
 __device__ __forceinline__ bool group_allsum(T (&v)[NV], Group& g, int slot) {
+  if (FORM == 3) return group_allsum_w0<NV, T>(v, g, slot);
   __shared__ double s_tot[NV];
   block_sum_to_thread0<NV, T>(v);
   if (g.nb == 1) {
@@ -216,7 +338,7 @@ __device__ __forceinline__ bool group_allsum(T (&v)[NV], Group& g, int slot) {
 #pragma unroll
     for (int m = 0; m < NV; ++m) g.part[(size_t)(slot + m) * g.nb + g.bid] = (double)v[m];
   }
-  const bool ok = group_barrier<FORM>(g);
+  const bool ok = group_barrier<(FORM >= 3 ? 1 : FORM)>(g);
   // Stage the NV x nb partials in shared memory with independent loads (all
   // in flight at once), then fold them in the fixed order: lane l of warp 0
   // sums partials l, l+32, ... sequentially, and the lanes are folded by the

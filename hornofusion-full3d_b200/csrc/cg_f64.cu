@@ -37,10 +37,6 @@ MeshDims make_dims(int nr, int nth, int nz) {
 
 namespace {
 
-constexpr int kUnroll = 2;   // cells per thread per round (streaming phases)
-constexpr int kUnrollA = 1;  // cells per thread per round (stencil phase)
-constexpr int kMaxBlock = 1024;
-
 struct CgArgs {
   MeshDims d;
   SysF64 s;
@@ -57,7 +53,9 @@ struct CgArgs {
 // out-of-slice lanes masked. Dead lanes add +0.0 to the dot sums, which
 // leaves them bit-identical to sums over the live cells alone.
 
-template <bool SYM>
+// U: cells per thread per round of the streaming phases; UA: of the stencil
+// phase. Kernels pick them by their register budget.
+template <bool SYM, int U, int UA>
 __device__ void cg_body(const CgArgs& a, Group& g) {
   const MeshDims& d = a.d;
   const SysF64& s = a.s;
@@ -77,17 +75,17 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
   double v3[3] = {0.0, 0.0, 0.0};
   {
     double* __restrict__ p0 = s.p;
-    for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnroll) {
-      double bv[kUnroll], rv[kUnroll], dv[kUnroll];
+    for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * U) {
+      double bv[U], rv[U], dv[U];
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
+      for (int u = 0; u < U; ++u) {
         const int c = min(c0 + u * B, last);
         bv[u] = b[c];
         rv[u] = r[c];
         dv[u] = aP[c];
       }
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
+      for (int u = 0; u < U; ++u) {
         const bool live = c0 + u * B < own.end;
         const double zv = rv[u] / guard_small(fabs(dv[u]));
         if (live) p0[c0 + u * B] = zv;
@@ -118,16 +116,16 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
       double* __restrict__ pcur = (iter & 1) ? s.p : s.p2;
       double v1[1] = {0.0};
       if (iter == 1) {
-        for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnrollA) {
-          double qv[kUnrollA], pc[kUnrollA];
+        for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * UA) {
+          double qv[UA], pc[UA];
 #pragma unroll
-          for (int u = 0; u < kUnrollA; ++u) {
+          for (int u = 0; u < UA; ++u) {
             const int c = min(c0 + u * B, last);
             pc[u] = pcur[c];
             qv[u] = apply_row<SYM, double>(d, A, pcur, c);
           }
 #pragma unroll
-          for (int u = 0; u < kUnrollA; ++u) {
+          for (int u = 0; u < UA; ++u) {
             const bool live = c0 + u * B < own.end;
             if (live) q[c0 + u * B] = qv[u];
             v1[0] = v1[0] + (live ? pc[u] * qv[u] : 0.0);
@@ -136,16 +134,16 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
       } else {
         const double bt = beta;
         auto pnew = [z, pold, bt](int cc) { return z[cc] + bt * pold[cc]; };
-        for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnrollA) {
-          double qv[kUnrollA], pc[kUnrollA];
+        for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * UA) {
+          double qv[UA], pc[UA];
 #pragma unroll
-          for (int u = 0; u < kUnrollA; ++u) {
+          for (int u = 0; u < UA; ++u) {
             const int c = min(c0 + u * B, last);
             pc[u] = pnew(c);
             qv[u] = apply_row_with<SYM, double>(d, A, pc[u], pnew, c);
           }
 #pragma unroll
-          for (int u = 0; u < kUnrollA; ++u) {
+          for (int u = 0; u < UA; ++u) {
             const bool live = c0 + u * B < own.end;
             if (live) {
               pcur[c0 + u * B] = pc[u];
@@ -161,10 +159,10 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
       const double alpha = rz / pq;
       // Phase B: phi += alpha pv; r -= alpha q; r.r; z and r.z (:538-553)
       double v2[2] = {0.0, 0.0};
-      for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * kUnroll) {
-        double pv[kUnroll], qv[kUnroll], dv[kUnroll], xv[kUnroll], rv[kUnroll];
+      for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * U) {
+        double pv[U], qv[U], dv[U], xv[U], rv[U];
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
+        for (int u = 0; u < U; ++u) {
           const int c = min(c0 + u * B, last);
           pv[u] = pcur[c];
           qv[u] = q[c];
@@ -173,7 +171,7 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
           rv[u] = r[c];
         }
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
+        for (int u = 0; u < U; ++u) {
           const bool live = c0 + u * B < own.end;
           const double xn = xv[u] + alpha * pv[u];
           const double rn = rv[u] - alpha * qv[u];
@@ -218,7 +216,13 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
   }
 }
 
-__global__ void __launch_bounds__(kMaxBlock) cg_f64_kernel(CgArgs a) {
+// Single-system kernel variants: the register budget per thread follows the
+// block size (64 at 1024 threads, 128 at 512, 255 at 256), and the larger
+// budgets carry more cells per round. Every variant owns the same slices and
+// visits a thread's cells in the same order, so all give the same bits for
+// one launch shape.
+template <int MAXB, int U, int UA>
+__global__ void __launch_bounds__(MAXB, 1) cg_f64_kernel(CgArgs a) {
   Group g;
   g.counter = a.ws.counter;
   g.err = a.ws.err;
@@ -229,9 +233,9 @@ __global__ void __launch_bounds__(kMaxBlock) cg_f64_kernel(CgArgs a) {
   g.timeout_ns = a.timeout_ns;
   g.epoch = 0;
   if (*a.s.asym == 0)
-    cg_body<true>(a, g);
+    cg_body<true, U, UA>(a, g);
   else
-    cg_body<false>(a, g);
+    cg_body<false, U, UA>(a, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -245,7 +249,11 @@ struct BatchF64Args {
   uint64_t timeout_ns;
 };
 
-__global__ void __launch_bounds__(kMaxBlock) batch_f64_kernel(BatchF64Args a) {
+// Blocks of kBatchBlock threads, two per SM (64 registers a thread): a batch
+// is throughput-bound over many small systems, so co-resident lanes count
+// for more than per-lane speed (the 128-register form with one block per SM
+// ran the 96-system mix 12 % slower).
+__global__ void __launch_bounds__(kBatchBlock, 2) batch_f64_kernel(BatchF64Args a) {
   const int lane = a.t.lane_of_block[blockIdx.x];
   const int first = a.t.lane_first_block[lane];
   Group g;
@@ -271,9 +279,9 @@ __global__ void __launch_bounds__(kMaxBlock) batch_f64_kernel(BatchF64Args a) {
     ca.tol = a.tol;
     ca.timeout_ns = a.timeout_ns;
     if (*bs.s.asym == 0)
-      cg_body<true>(ca, g);
+      cg_body<true, 2, 1>(ca, g);
     else
-      cg_body<false>(ca, g);
+      cg_body<false, 2, 1>(ca, g);
   }
 }
 
@@ -424,11 +432,16 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
-  return cudaLaunchCooperativeKernel((const void*)cg_f64_kernel, dim3(grid),
-                                     dim3(block), args, 0, st);
+  return cudaLaunchCooperativeKernel(cg_f64_kernel_ptr(block), dim3(grid), dim3(block),
+                                     args, 0, st);
 }
 
-const void* cg_f64_kernel_ptr() { return (const void*)cg_f64_kernel; }
+const void* cg_f64_kernel_ptr(int block) {
+  if (block <= 256) return (const void*)cg_f64_kernel<256, 4, 4>;
+  if (block <= 512) return (const void*)cg_f64_kernel<512, 4, 2>;
+  return (const void*)cg_f64_kernel<1024, 2, 1>;
+}
+
 
 cudaError_t launch_batch_f64(const BatchTables& t, int grid, int block, int max_iter,
                              double tol, uint64_t timeout_ns, cudaStream_t st) {

@@ -58,6 +58,7 @@ struct GroupWs {
 
 MeshDims make_dims(int nr, int nth, int nz);
 
+
 // pack: halo layout -> compact layout, symmetry check, FP64 initial
 // residual r = Su - A phi with the reference stencil (phi's theta halo
 // wrapped, its r/z halo cells read as given).
@@ -71,7 +72,9 @@ cudaError_t launch_unpack_f64(const MeshDims& d, const double* x, double* phi,
 cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
                           int max_iter, double tol, uint64_t timeout_ns,
                           int grid, int block, cudaStream_t st);
-const void* cg_f64_kernel_ptr();
+// The single-system kernel variant that runs blocks of `block` threads.
+const void* cg_f64_kernel_ptr(int block);
+
 
 
 
@@ -115,6 +118,8 @@ cudaError_t launch_batch_mixed(const BatchTables& t, int grid, int block,
                                int max_outer, int max_inner, double tol,
                                double inner_tol, uint64_t timeout_ns, cudaStream_t st);
 const void* batch_f64_kernel_ptr();
+// Threads per block of the batched kernels (FP64 and mixed).
+constexpr int kBatchBlock = 512;
 const void* batch_mixed_kernel_ptr();
 
 // Barrier self-test (api.cu).

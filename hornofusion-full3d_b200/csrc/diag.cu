@@ -39,7 +39,7 @@ extern "C" int eaf_diag_allreduce_us(int device, int blocks, int threads, int it
                                      int form, double* us_per_allreduce) {
   if (!us_per_allreduce || blocks < 1 || blocks > eaf::kMaxGroupBlocks ||
       threads < 64 || threads > 1024 || threads % 32 || iters < 1 || form < 0 ||
-      form > 2)
+      form > 3)
     return EAF_EINVAL;
   eaf::DeviceGuard guard(device);
   if (!guard.ok()) return EAF_ECUDA;
@@ -56,7 +56,8 @@ extern "C" int eaf_diag_allreduce_us(int device, int blocks, int threads, int it
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   const void* kern = form == 0   ? (const void*)eaf::allreduce_bench_kernel<0>
                      : form == 1 ? (const void*)eaf::allreduce_bench_kernel<1>
-                                 : (const void*)eaf::allreduce_bench_kernel<2>;
+                     : form == 2 ? (const void*)eaf::allreduce_bench_kernel<2>
+                                 : (const void*)eaf::allreduce_bench_kernel<3>;
   uint64_t timeout = 2000ull * 1000ull * 1000ull;
   float ms = 0.f;
   for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {  // rep 0 warms up

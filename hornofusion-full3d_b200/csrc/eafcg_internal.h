@@ -44,6 +44,5 @@ int plan_lanes(const std::vector<int>& widths, const std::vector<long long>& cel
 double model_solve_us(long long cells, int w);
 BatchTables tables_from(const int* d_tab, int grid, int nlanes, const BatchSys* d_sys,
                         unsigned long long* counters, double* parts, int* err);
-constexpr int kBatchBlock = 512;
 
 }  // namespace eaf

@@ -31,11 +31,11 @@ struct TunedLaunch {
 
 // (block, grid) of the single-system persistent solver.
 static const TunedLaunch kTunedLaunches[] = {
-    {12, 24, 16, 256, 18},
+    {12, 24, 16, 256, 9},
     {18, 36, 24, 256, 32},
     {35, 70, 50, 512, 148},
-    {60, 120, 84, 1024, 148},
-    {120, 240, 168, 1024, 148},
+    {60, 120, 84, 512, 148},
+    {120, 240, 168, 512, 148},
 };
 
 inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid) {

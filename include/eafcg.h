@@ -280,8 +280,10 @@ int eaf_selftest_barrier_timeout(int device, double timeout_ms);
 /* Diagnostics (no reference counterpart): device time of one group
  * all-reduce of two sums -- block reduction, bounded group barrier, staging
  * and fold of the block partials -- averaged over `iters` in one cooperative
- * launch of blocks x threads, with barrier memory-ordering form 0, 1 or 2
- * (the solvers use form 1). */
+ * launch of blocks x threads, in form 0, 1 or 2 (full block barriers around
+ * a counter barrier with three memory-ordering variants) or 3 (warp 0
+ * exchanges while the other warps wait once on a named barrier; the form
+ * the solvers use). All forms fold in the same order. */
 int eaf_diag_allreduce_us(int device, int blocks, int threads, int iters,
                           int form, double* us_per_allreduce);
 
