@@ -115,8 +115,8 @@ static int max_coresident(const void* kernel, int block, int sms) {
 // 2048 cells; capped by co-residency of the kernel (variant) that runs
 // blocks of that size.
 static void pick_launch(const eaf_cg* h, bool f64, int* grid, int* block) {
-  auto kernel_for = [f64](int b) {
-    return f64 ? eaf::cg_f64_kernel_ptr(b) : eaf::cg_mixed_kernel_ptr();
+  auto kernel_for = [f64, h](int b) {
+    return f64 ? eaf::cg_f64_kernel_ptr(b, h->d.n) : eaf::cg_mixed_kernel_ptr();
   };
   int b = h->block > 0 ? h->block : kDefaultBlock;
   int g;

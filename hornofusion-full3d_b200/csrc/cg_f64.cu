@@ -37,6 +37,23 @@ MeshDims make_dims(int nr, int nth, int nz) {
 
 namespace {
 
+// Bulk L2 prefetch (the TMA unit's cp.async.bulk.prefetch.L2) of cells
+// [lo, hi) of array a, clamped to [0, n) and to 16-byte boundaries inside the
+// array; a hint with no register or ordering cost.
+__device__ __forceinline__ void l2_prefetch_cells(const double* a, int lo, int hi, int n) {
+  lo = max(lo, 0);
+  hi = min(hi, n);
+  if (hi <= lo) return;
+  const uintptr_t base = (uintptr_t)a;
+  const uintptr_t b = ((uintptr_t)(a + lo)) & ~(uintptr_t)15;
+  uintptr_t e = ((uintptr_t)(a + hi) + 15) & ~(uintptr_t)15;
+  const uintptr_t end = (base + (uintptr_t)n * 8) & ~(uintptr_t)15;
+  if (e > end) e = end;
+  if (b < base || e <= b) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((unsigned)(e - b))
+               : "memory");
+}
+
 struct CgArgs {
   MeshDims d;
   SysF64 s;
@@ -54,8 +71,10 @@ struct CgArgs {
 // leaves them bit-identical to sums over the live cells alone.
 
 // U: cells per thread per round of the streaming phases; UA: of the stencil
-// phase. Kernels pick them by their register budget.
-template <bool SYM, int U, int UA>
+// phase. Kernels pick them by their register budget. PF: threads 0..7 of the
+// block prefetch the block's next round of every streamed array into L2
+// (one bulk prefetch per array), for meshes whose working set exceeds L2.
+template <bool SYM, int U, int UA, bool PF>
 __device__ void cg_body(const CgArgs& a, Group& g) {
   const MeshDims& d = a.d;
   const SysF64& s = a.s;
@@ -117,6 +136,12 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
       double v1[1] = {0.0};
       if (iter == 1) {
         for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * UA) {
+          if (PF && threadIdx.x < 6) {
+            const int nl = c0 - (int)threadIdx.x + B * UA, nh = min(nl + B * UA, own.end);
+            const double* arr[6] = {pcur, aP, A.aE, A.aN, A.aT, pcur};
+            const int off = threadIdx.x == 5 ? d.plane : 0;
+            l2_prefetch_cells(arr[threadIdx.x], nl + off, nh + off, d.n);
+          }
           double qv[UA], pc[UA];
 #pragma unroll
           for (int u = 0; u < UA; ++u) {
@@ -135,6 +160,12 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
         const double bt = beta;
         auto pnew = [z, pold, bt](int cc) { return z[cc] + bt * pold[cc]; };
         for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * UA) {
+          if (PF && threadIdx.x < 8) {
+            const int nl = c0 - (int)threadIdx.x + B * UA, nh = min(nl + B * UA, own.end);
+            const double* arr[8] = {z, pold, aP, A.aE, A.aN, A.aT, z, pold};
+            const int off = threadIdx.x >= 6 ? d.plane : 0;
+            l2_prefetch_cells(arr[threadIdx.x], nl + off, nh + off, d.n);
+          }
           double qv[UA], pc[UA];
 #pragma unroll
           for (int u = 0; u < UA; ++u) {
@@ -160,6 +191,11 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
       // Phase B: phi += alpha pv; r -= alpha q; r.r; z and r.z (:538-553)
       double v2[2] = {0.0, 0.0};
       for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * U) {
+        if (PF && threadIdx.x < 5) {
+          const int nl = c0 - (int)threadIdx.x + B * U, nh = min(nl + B * U, own.end);
+          const double* arr[5] = {pcur, q, aP, x, r};
+          l2_prefetch_cells(arr[threadIdx.x], nl, nh, d.n);
+        }
         double pv[U], qv[U], dv[U], xv[U], rv[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -221,7 +257,7 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
 // budgets carry more cells per round. Every variant owns the same slices and
 // visits a thread's cells in the same order, so all give the same bits for
 // one launch shape.
-template <int MAXB, int U, int UA>
+template <int MAXB, int U, int UA, bool PF>
 __global__ void __launch_bounds__(MAXB, 1) cg_f64_kernel(CgArgs a) {
   Group g;
   g.counter = a.ws.counter;
@@ -233,9 +269,9 @@ __global__ void __launch_bounds__(MAXB, 1) cg_f64_kernel(CgArgs a) {
   g.timeout_ns = a.timeout_ns;
   g.epoch = 0;
   if (*a.s.asym == 0)
-    cg_body<true, U, UA>(a, g);
+    cg_body<true, U, UA, PF>(a, g);
   else
-    cg_body<false, U, UA>(a, g);
+    cg_body<false, U, UA, PF>(a, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -279,9 +315,9 @@ __global__ void __launch_bounds__(kBatchBlock, 2) batch_f64_kernel(BatchF64Args 
     ca.tol = a.tol;
     ca.timeout_ns = a.timeout_ns;
     if (*bs.s.asym == 0)
-      cg_body<true, 2, 1>(ca, g);
+      cg_body<true, 2, 1, false>(ca, g);
     else
-      cg_body<false, 2, 1>(ca, g);
+      cg_body<false, 2, 1, false>(ca, g);
   }
 }
 
@@ -432,14 +468,17 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
-  return cudaLaunchCooperativeKernel(cg_f64_kernel_ptr(block), dim3(grid), dim3(block),
-                                     args, 0, st);
+  return cudaLaunchCooperativeKernel(cg_f64_kernel_ptr(block, d.n), dim3(grid),
+                                     dim3(block), args, 0, st);
 }
 
-const void* cg_f64_kernel_ptr(int block) {
-  if (block <= 256) return (const void*)cg_f64_kernel<256, 4, 4>;
-  if (block <= 512) return (const void*)cg_f64_kernel<512, 4, 2>;
-  return (const void*)cg_f64_kernel<1024, 2, 1>;
+bool l2_prefetch_pays(long long n) { return (double)n * 128.0 > 96.0e6; }
+
+const void* cg_f64_kernel_ptr(int block, long long n) {
+  if (block <= 256) return (const void*)cg_f64_kernel<256, 4, 4, false>;
+  if (block <= 512) return (const void*)cg_f64_kernel<512, 4, 2, false>;
+  if (l2_prefetch_pays(n)) return (const void*)cg_f64_kernel<1024, 2, 1, true>;
+  return (const void*)cg_f64_kernel<1024, 2, 1, false>;
 }
 
 

@@ -72,8 +72,14 @@ cudaError_t launch_unpack_f64(const MeshDims& d, const double* x, double* phi,
 cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
                           int max_iter, double tol, uint64_t timeout_ns,
                           int grid, int block, cudaStream_t st);
-// The single-system kernel variant that runs blocks of `block` threads.
-const void* cg_f64_kernel_ptr(int block);
+// The single-system kernel variant that runs blocks of `block` threads on
+// an n-cell mesh. The 1024-thread variant prefetches into L2 ahead of its
+// load rounds when the mesh's working set (128 B a cell) is larger than the
+// L2 can hold alongside it (l2_prefetch_pays): at 64 registers it has too
+// few loads in flight to keep HBM busy on its own. All variants give the
+// same bits for one launch shape.
+bool l2_prefetch_pays(long long n);
+const void* cg_f64_kernel_ptr(int block, long long n);
 
 
 

@@ -81,7 +81,7 @@ cudaError_t scratch_on(int dev, double** out) {
 
 int max_coresident(int block, int dev) {
   int per_sm = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eaf::cg_f64_kernel_ptr(block),
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eaf::cg_f64_kernel_ptr(block, 0),
                                                     block, 0) != cudaSuccess)
     return 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)

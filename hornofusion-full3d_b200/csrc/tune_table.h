@@ -13,7 +13,7 @@ struct TunedWidth {
 static const TunedWidth kTunedWidths[] = {
     {12, 24, 16, 1},
     {18, 36, 24, 4},
-    {35, 70, 50, 32},
+    {35, 70, 50, 24},
     {60, 120, 84, 48},
 };
 
@@ -31,11 +31,11 @@ struct TunedLaunch {
 
 // (block, grid) of the single-system persistent solver.
 static const TunedLaunch kTunedLaunches[] = {
-    {12, 24, 16, 256, 9},
+    {12, 24, 16, 256, 8},
     {18, 36, 24, 256, 32},
-    {35, 70, 50, 512, 148},
+    {35, 70, 50, 256, 148},
     {60, 120, 84, 512, 148},
-    {120, 240, 168, 512, 148},
+    {120, 240, 168, 1024, 148},
 };
 
 inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid) {

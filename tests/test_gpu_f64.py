@@ -103,6 +103,17 @@ def test_production_mesh_fixed_iterations_bitwise(launch):
     assert nit == 150 and plan[0] > 1
 
 
+@pytest.mark.parametrize("launch", [(1024, 148), (512, 148)])
+def test_mesh_beyond_l2_fixed_iterations_bitwise(launch):
+    """100x100x80 (800,000 cells, working set beyond L2): at 1024 threads the
+    L2-prefetching kernel variant runs; bitwise against the oracle either way."""
+    g = gen()
+    s = g.make_system(100, 100, 80, 16, seed=2)
+    res, nit, st, plan, _ = assert_bitwise(s, g.zeros_phi(100, 100, 80),
+                                           max_iter=40, tol=0.0, launch=launch)
+    assert nit == 40 and plan == (148, launch[0])
+
+
 def test_production_mesh_to_tol_vs_sequential_oracle():
     """60x120x84 to 1e-8 against the threaded sequential-association oracle."""
     import oracle
