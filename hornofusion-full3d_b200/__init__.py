@@ -107,6 +107,28 @@ class CGSolver:
         check(st, "eaf_cg_solve_f64", allow=(EAF_OK, EAF_ENONFINITE))
         return res.value, nit.value, st
 
+    def tdma(self, arrays, phi, n_sweep: int, device_ptrs: bool = False) -> None:
+        """Line-by-line TDMA sweeps in place on phi (tdma_3d_mpi,
+        src/mod_solver_3d.f90:252-366): ``arrays`` = (aW, aE, aS, aN, aB, aT,
+        aP, Su) of any (not necessarily symmetric) transport equation."""
+        arrays = list(arrays)
+        self._check_shape(arrays + [phi])
+        fn = (self._lib.eaf_tdma_3d_f64_device if device_ptrs
+              else self._lib.eaf_tdma_3d_f64)
+        st = fn(self._h, *[_ptr(a) for a in arrays], _ptr(phi), int(n_sweep))
+        check(st, "eaf_tdma_3d_f64")
+
+    def residual(self, arrays, phi, device_ptrs: bool = False) -> float:
+        """compute_residual_3d_mpi (src/mod_solver_3d.f90:625-694)."""
+        arrays = list(arrays)
+        self._check_shape(arrays + [phi])
+        res = ctypes.c_double()
+        fn = (self._lib.eaf_residual_3d_f64_device if device_ptrs
+              else self._lib.eaf_residual_3d_f64)
+        st = fn(self._h, *[_ptr(a) for a in arrays], _ptr(phi), ctypes.byref(res))
+        check(st, "eaf_residual_3d_f64")
+        return res.value
+
     def solve_mixed(self, arrays, phi, tol: float = SOR_TOL_PRESSURE,
                     inner_tol: float = 0.1, max_outer: int = 200,
                     max_inner: int = 100000, device_ptrs: bool = False):

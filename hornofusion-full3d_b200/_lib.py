@@ -54,6 +54,10 @@ SIGNATURES = [
     ("eaf_cg_destroy", _ci, [_vp]),
     ("eaf_cg_solve_f64", _ci, [_vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
     ("eaf_cg_solve_f64_device", _ci, [_vp] + _A8 + [_vp, _ci, _cd, _pd, _pi]),
+    ("eaf_tdma_3d_f64", _ci, [_vp] + _A8 + [_vp, _ci]),
+    ("eaf_tdma_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _ci]),
+    ("eaf_residual_3d_f64", _ci, [_vp] + _A8 + [_vp, _pd]),
+    ("eaf_residual_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _pd]),
     ("eaf_cg_solve_mixed", _ci,
      [_vp] + _A8 + [_vp, _ci, _ci, _cd, _cd, _pd, _pi, _pi]),
     ("eaf_cg_solve_mixed_device", _ci,
@@ -71,6 +75,9 @@ SIGNATURES = [
     ("eaf_host_unregister", _ci, [_vp]),
     ("eaf_selftest_barrier_timeout", _ci, [_ci, _cd]),
     ("eaf_diag_allreduce_us", _ci, [_ci, _ci, _ci, _ci, _ci, _pd]),
+    ("eaf_diag_div_check", _ci, [_ci, ctypes.c_longlong, ctypes.c_ulonglong,
+                                 ctypes.POINTER(ctypes.c_longlong),
+                                 ctypes.POINTER(ctypes.c_longlong)]),
     ("eaf_batch_create", _ci, [ctypes.POINTER(_vp), _ci, _pi, _ci]),
     ("eaf_batch_destroy", _ci, [_vp]),
     ("eaf_batch_set_width", _ci, [_vp, _ci, _ci]),

@@ -36,6 +36,7 @@ UNITS = {
     "noalloc.cu": ["-fmad=false"],
     "serve.cu": [],
     "diag.cu": [],
+    "tdma.cu": ["-fmad=false"],
 }
 
 

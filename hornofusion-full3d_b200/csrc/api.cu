@@ -46,6 +46,8 @@ struct eaf_cg {
   double last_solve_ms, last_kernel_ms, last_e2e_ms;
   int last_sym, last_kernels;
   int last_grid, last_block;
+  int* tdma_prog;    // per-owner progress of the TDMA sweeps (lazy)
+  double* tdma_fac;  // TDMA line factors (lazy)
 };
 
 namespace eaf {
@@ -95,6 +97,8 @@ static void free_handle(eaf_cg* h) {
   cudaFree(h->ws.counter);
   cudaFree(h->ws.err);
   cudaFree(h->ws.result);
+  cudaFree(h->tdma_prog);
+  cudaFree(h->tdma_fac);
   if (h->res_h) cudaFreeHost(h->res_h);
   for (int i = 0; i < 6; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -414,6 +418,75 @@ int solve_host(eaf_cg* h, const double* const arr[8], double* phi, const SolveOp
   return finish_solve(h, true, residual, n_iter, n_outer);
 }
 
+// ---------------------------------------------------------------------------
+// Line-by-line TDMA sweeps and the transport residual on the handle's mesh.
+// ---------------------------------------------------------------------------
+int enqueue_tdma(eaf_cg* h, const HaloInputs& in, double* phi, int n_sweep) {
+  if (!h->tdma_prog) {
+    EAF_CUDA(cudaMalloc((void**)&h->tdma_prog, sizeof(int) * eaf::tdma_progress_ints()));
+  }
+  if (!h->tdma_fac) {
+    EAF_CUDA(cudaMalloc((void**)&h->tdma_fac,
+                        sizeof(double) * eaf::tdma_factor_doubles(h->nr, h->nth, h->nz)));
+  }
+  h->last_grid = eaf::tdma_grid(h->nr, h->nth, h->nz);
+  h->last_block = 32;
+  EAF_CUDA(cudaEventRecord(h->ev[1], h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
+  if (n_sweep > 0) {
+    EAF_CUDA(eaf::launch_tdma_f64(in, phi, h->nr, h->nth, h->nz, n_sweep, h->tdma_prog,
+                                  h->tdma_fac, h->ws, h->timeout_ns, h->st));
+  }
+  EAF_CUDA(cudaEventRecord(h->ev[3], h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[4], h->st));
+  h->last_kernels = n_sweep > 0 ? 2 : 0;
+  return EAF_OK;
+}
+
+int finish_tdma(eaf_cg* h, bool host_path, int n_sweep) {
+  int err = 0;
+  if (n_sweep > 0)
+    EAF_CUDA(cudaMemcpyAsync(&h->res_h->status, h->ws.err, sizeof(int),
+                             cudaMemcpyDeviceToHost, h->st));
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  if (n_sweep > 0) err = h->res_h->status;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[1], h->ev[4]) == cudaSuccess) h->last_solve_ms = ms;
+  if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
+  if (host_path && cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]) == cudaSuccess)
+    h->last_e2e_ms = ms;
+  return err;
+}
+
+int residual_launch_shape(const eaf_cg* h, int* grid, int* block) {
+  const int b = 512;
+  long long g = ((long long)h->d.n + 4095) / 4096;
+  if (g < 1) g = 1;
+  if (g > h->sms) g = h->sms;
+  *grid = (int)g;
+  *block = b;
+  return EAF_OK;
+}
+
+int run_residual(eaf_cg* h, const HaloInputs& in, const double* phi, double* residual) {
+  int grid, block;
+  residual_launch_shape(h, &grid, &block);
+  h->last_grid = grid;
+  h->last_block = block;
+  EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
+  EAF_CUDA(eaf::launch_residual_f64(in, phi, h->d, h->ws, h->timeout_ns, grid, block,
+                                    h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[3], h->st));
+  EAF_CUDA(cudaMemcpyAsync(h->res_h, h->ws.result, sizeof(SolveResult),
+                           cudaMemcpyDeviceToHost, h->st));
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
+  h->last_kernels = 1;
+  *residual = h->res_h->residual;
+  return h->res_h->status;
+}
+
 }  // namespace
 
 extern "C" {
@@ -492,6 +565,66 @@ int eaf_selftest_barrier_timeout(int device, double timeout_ms) {
     return EAF_ECUDA;
   }
   return err_h;
+}
+
+int eaf_tdma_3d_f64(eaf_cg_t h, const double* aW, const double* aE, const double* aS,
+                    const double* aN, const double* aB, const double* aT,
+                    const double* aP, const double* Su, double* phi, int n_sweep) {
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  if (!h || !phi || any_null(arr, 8)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  const size_t bytes = h->nh * sizeof(double);
+  EAF_CUDA(cudaEventRecord(h->ev[0], h->st));
+  for (int i = 0; i < 8; ++i)
+    EAF_CUDA(cudaMemcpyAsync(h->stage[i], arr[i], bytes, cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(h->stage[8], phi, bytes, cudaMemcpyHostToDevice, h->st));
+  HaloInputs in = {h->stage[0], h->stage[1], h->stage[2], h->stage[3], h->stage[4],
+                   h->stage[5], h->stage[6], h->stage[7], h->stage[8]};
+  int rc = enqueue_tdma(h, in, h->stage[8], n_sweep);
+  if (rc != EAF_OK) return rc;
+  EAF_CUDA(cudaMemcpyAsync(phi, h->stage[8], bytes, cudaMemcpyDeviceToHost, h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[5], h->st));
+  return finish_tdma(h, true, n_sweep);
+}
+
+int eaf_tdma_3d_f64_device(eaf_cg_t h, const double* aW, const double* aE,
+                           const double* aS, const double* aN, const double* aB,
+                           const double* aT, const double* aP, const double* Su,
+                           double* phi, int n_sweep) {
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  if (!h || !phi || any_null(arr, 8)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  HaloInputs in = {arr[0], arr[1], arr[2], arr[3], arr[4], arr[5], arr[6], arr[7], phi};
+  int rc = enqueue_tdma(h, in, phi, n_sweep);
+  if (rc != EAF_OK) return rc;
+  return finish_tdma(h, false, n_sweep);
+}
+
+int eaf_residual_3d_f64(eaf_cg_t h, const double* aW, const double* aE, const double* aS,
+                        const double* aN, const double* aB, const double* aT,
+                        const double* aP, const double* Su, const double* phi,
+                        double* residual) {
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  if (!h || !phi || !residual || any_null(arr, 8)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  const size_t bytes = h->nh * sizeof(double);
+  for (int i = 0; i < 8; ++i)
+    EAF_CUDA(cudaMemcpyAsync(h->stage[i], arr[i], bytes, cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(h->stage[8], phi, bytes, cudaMemcpyHostToDevice, h->st));
+  HaloInputs in = {h->stage[0], h->stage[1], h->stage[2], h->stage[3], h->stage[4],
+                   h->stage[5], h->stage[6], h->stage[7], h->stage[8]};
+  return run_residual(h, in, h->stage[8], residual);
+}
+
+int eaf_residual_3d_f64_device(eaf_cg_t h, const double* aW, const double* aE,
+                               const double* aS, const double* aN, const double* aB,
+                               const double* aT, const double* aP, const double* Su,
+                               const double* phi, double* residual) {
+  const double* arr[8] = {aW, aE, aS, aN, aB, aT, aP, Su};
+  if (!h || !phi || !residual || any_null(arr, 8)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  HaloInputs in = {arr[0], arr[1], arr[2], arr[3], arr[4], arr[5], arr[6], arr[7], phi};
+  return run_residual(h, in, phi, residual);
 }
 
 }  // extern "C"

@@ -124,6 +124,28 @@ cudaError_t launch_batch_mixed(const BatchTables& t, int grid, int block,
                                int max_outer, int max_inner, double tol,
                                double inner_tol, uint64_t timeout_ns, cudaStream_t st);
 const void* batch_f64_kernel_ptr();
+// Line-by-line TDMA sweeps (tdma_3d_mpi, serial) on halo-layout arrays, in
+// place on phi; `prog` holds tdma_progress_ints() ints of per-owner
+// progress. One cooperative launch of tdma_grid() warps.
+// `fac` holds tdma_factor_doubles() doubles of line factors (computed by the
+// launch from the coefficients).
+size_t tdma_progress_ints();
+size_t tdma_factor_doubles(int nr, int nth, int nz);
+int tdma_grid(int nr, int nth, int nz);
+cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, int nz,
+                            int n_sweep, int* prog, double* fac, const GroupWs& ws,
+                            uint64_t timeout_ns, cudaStream_t st);
+const void* tdma_kernel_ptr();
+// compute_residual_3d_mpi (serial) into ws.result->residual.
+cudaError_t launch_residual_f64(const HaloInputs& in, const double* phi, const MeshDims& d,
+                                const GroupWs& ws, uint64_t timeout_ns, int grid, int block,
+                                cudaStream_t st);
+const void* residual_kernel_ptr();
+// Counts[0] = pairs where the TDMA's reciprocal-corrected division differs
+// from `/` in any bit, counts[1] = pairs that took its fast path.
+cudaError_t run_div_check(long long n, unsigned long long seed, unsigned long long* counts,
+                          cudaStream_t st);
+
 // Threads per block of the batched kernels (FP64 and mixed).
 constexpr int kBatchBlock = 512;
 const void* batch_mixed_kernel_ptr();

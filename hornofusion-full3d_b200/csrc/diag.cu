@@ -87,3 +87,23 @@ extern "C" int eaf_diag_allreduce_us(int device, int blocks, int threads, int it
   *us_per_allreduce = 1.0e3 * ms / iters;
   return err_h;
 }
+
+extern "C" int eaf_diag_div_check(int device, long long n, unsigned long long seed,
+                                  long long* mismatches, long long* fast_path) {
+  if (n < 1 || !mismatches || !fast_path) return EAF_EINVAL;
+  eaf::DeviceGuard guard(device);
+  if (!guard.ok()) return EAF_ECUDA;
+  unsigned long long* d = nullptr;
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = cudaMalloc((void**)&d, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = eaf::run_div_check(n, seed, d, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    eaf::set_error("eaf_diag_div_check", e);
+    return EAF_ECUDA;
+  }
+  *mismatches = (long long)h[0];
+  *fast_path = (long long)h[1];
+  return EAF_OK;
+}

@@ -267,6 +267,67 @@ def apply_operator(s: System, x_h: np.ndarray) -> np.ndarray:
             - I(s.aN) * xn - I(s.aB) * xb - I(s.aT) * xt)
 
 
+def make_transport_system(nr: int, nth: int, nz: int, seed: int = 0,
+                          trivial_frac: float = 0.05, peclet: float = 2.0,
+                          sp_frac: float = 0.1) -> System:
+    """A seeded transport-equation system of the kind the line-by-line TDMA
+    (tdma_3d_mpi) solves for momentum, energy and species: upwind-style
+    links a_E = D_e + max(-F_e, 0), a_W = D_w + max(F_w, 0) (likewise S/N,
+    B/T) from per-face diffusion D ~ U[0.5, 1.5] and flux F ~ N(0, peclet/2),
+    so the operator is asymmetric; walls zeroed at the axis (i = 1, W), the
+    shell (i = nr, E), the floor (k = 1, B) and the roof (k = nz, T); theta
+    periodic; a_P = (sum of links) * (1 + U[0, sp_frac]) (diagonally
+    dominant, so the sweeps converge); Su ~ N(0, 1). A fraction
+    `trivial_frac` of the cells are identity rows (a_P = 1, links 0, Su = 0),
+    the form the reference's inactive cells take. Halos are zero."""
+    rng = np.random.default_rng(seed)
+    shp = (nz, nth, nr)
+
+    def links(axis_len, faces_shape, periodic):
+        D = rng.uniform(0.5, 1.5, size=faces_shape)
+        F = rng.normal(0.0, peclet / 2.0, size=faces_shape)
+        if not periodic:
+            idx = [slice(None)] * 3
+            ax = {"z": 0, "t": 1, "r": 2}[axis_len]
+            idx[ax] = 0
+            D[tuple(idx)] = 0.0
+            F[tuple(idx)] = 0.0
+            idx[ax] = -1
+            D[tuple(idx)] = 0.0
+            F[tuple(idx)] = 0.0
+        return D, F
+
+    # faces: r has nr+1 (axis .. shell), theta nth (periodic), z nz+1
+    Dr, Fr = links("r", (nz, nth, nr + 1), False)
+    Dt, Ft = links("t", (nz, nth, nr), True)
+    Dz, Fz = links("z", (nz + 1, nth, nr), False)
+    aW = Dr[:, :, :-1] + np.maximum(Fr[:, :, :-1], 0.0)
+    aE = Dr[:, :, 1:] + np.maximum(-Fr[:, :, 1:], 0.0)
+    # theta face j+1/2 stored at index j; the south face of j is face j-1/2
+    Dt_s, Ft_s = np.roll(Dt, 1, axis=1), np.roll(Ft, 1, axis=1)
+    aS = Dt_s + np.maximum(Ft_s, 0.0)
+    aN = Dt + np.maximum(-Ft, 0.0)
+    aB = Dz[:-1] + np.maximum(Fz[:-1], 0.0)
+    aT = Dz[1:] + np.maximum(-Fz[1:], 0.0)
+    aW[:, :, 0] = 0.0
+    aE[:, :, -1] = 0.0
+    aB[0] = 0.0
+    aT[-1] = 0.0
+    tot = ((((aW + aE) + aS) + aN) + aB) + aT
+    aP = tot * (1.0 + rng.uniform(0.0, sp_frac, size=shp))
+    Su = rng.normal(0.0, 1.0, size=shp)
+    triv = rng.random(shp) < trivial_frac
+    for a in (aW, aE, aS, aN, aB, aT, Su):
+        a[triv] = 0.0
+    aP[triv] = 1.0
+    out = {}
+    for name, a in zip(COEF_NAMES, (aW, aE, aS, aN, aB, aT, aP, Su)):
+        h = zeros_phi(nr, nth, nz)
+        interior(h)[...] = a
+        out[name] = h
+    return System(nr=nr, nth=nth, nz=nz, **out)
+
+
 def system_bytes(nr: int, nth: int, nz: int) -> int:
     """Host bytes of one system (8 halo-layout FP64 arrays)."""
     return 8 * 8 * (nr + 4) * (nth + 4) * (nz + 4)

@@ -28,9 +28,14 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=0,
                     help="solve this many copies of the mixed batch instead "
                          "(12x24x16, 18x36x24, 35x70x50, 60x120x84 round robin)")
+    ap.add_argument("--tdma", type=int, default=0,
+                    help="time this many line-TDMA sweeps of a transport system "
+                         "on the mesh instead of a CG solve")
     args = ap.parse_args(argv)
     if args.batch:
         return batch_case(args)
+    if args.tdma:
+        return tdma_case(args)
     import torch
     eaf = importlib.import_module("hornofusion-full3d_b200")
     g = importlib.import_module("hornofusion-full3d_b200.eafgen")
@@ -59,6 +64,30 @@ def main(argv=None):
                         "us_per_iter": 1e3 * t["kernel_ms"] / max(nit, 1)})
     print(json.dumps({"mesh": [nr, nth, nz], "launch": [grid, block],
                       "mixed": args.mixed, "runs": out}))
+    return 0
+
+
+def tdma_case(args):
+    import torch
+    eaf = importlib.import_module("hornofusion-full3d_b200")
+    g = importlib.import_module("hornofusion-full3d_b200.eafgen")
+    nr, nth, nz = args.mesh
+    s = g.make_transport_system(nr, nth, nz, seed=0)
+    dev = [torch.from_numpy(a).cuda() for a in s.arrays()]
+    phi = torch.zeros(g.halo_shape(nr, nth, nz), dtype=torch.float64, device="cuda")
+    out = []
+    with eaf.CGSolver(nr, nth, nz) as cg:
+        for _ in range(args.repeat):
+            phi.zero_()
+            torch.cuda.synchronize()
+            cg.tdma(dev, phi, args.tdma, device_ptrs=True)
+            t = cg.last_timing()
+            out.append({"sweeps": args.tdma, "kernel_ms": t["kernel_ms"],
+                        "ms_per_sweep": t["kernel_ms"] / args.tdma,
+                        "ns_per_cell_sweep": 1e6 * t["kernel_ms"] / args.tdma
+                        / (nr * nth * nz)})
+        launch = cg.last_launch()
+    print(json.dumps({"mesh": [nr, nth, nz], "tdma": True, "launch": launch, "runs": out}))
     return 0
 
 

@@ -128,6 +128,41 @@ int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks);
  * dot products; the oracle's kernel-order mode takes the same shape). */
 int eaf_cg_last_launch(eaf_cg_t h, int* block_threads, int* grid_blocks);
 
+/* Line-by-line TDMA on the handle's mesh: replaces tdma_3d_mpi
+ * (src/mod_solver_3d.f90:252-366, serial branch; callers in momentum,
+ * energy, species, k-epsilon, DO radiation and continuity, e.g.
+ * src/mod_momentum_3d.f90:329). n_sweep sweeps of Thomas line solves -- all r
+ * lines, then all theta lines, then all z lines, theta halos refreshed
+ * before each direction -- in the reference's Gauss-Seidel line order, so
+ * phi comes out bit-identical to the sequential routine. The eight inputs
+ * and phi are in the CG's halo layout; phi is updated in place (interior and
+ * theta halos). Works on any linear operator (the transport equations are
+ * not symmetric). n_sweep <= 0 leaves phi untouched. Returns EAF_OK,
+ * EAF_ETIMEOUT (a bounded wait between lines gave up), EAF_EINVAL or
+ * EAF_ECUDA. */
+int eaf_tdma_3d_f64(eaf_cg_t h, const double* aW, const double* aE, const double* aS,
+                    const double* aN, const double* aB, const double* aT,
+                    const double* aP, const double* Su, double* phi, int n_sweep);
+int eaf_tdma_3d_f64_device(eaf_cg_t h, const double* aW, const double* aE,
+                           const double* aS, const double* aN, const double* aB,
+                           const double* aT, const double* aP, const double* Su,
+                           double* phi, int n_sweep);
+
+/* Relative residual of a transport equation: replaces
+ * compute_residual_3d_mpi (src/mod_solver_3d.f90:625-694, serial):
+ * sqrt(sum r^2) / (sqrt(sum (|Su| + |aP phi| + SMALL)^2) + SMALL) over the
+ * cells that are not identity rows, phi's halos read as stored. The two sums
+ * are associated as the CG's dot products for the launch shape reported by
+ * eaf_cg_last_launch (the reference sums sequentially). */
+int eaf_residual_3d_f64(eaf_cg_t h, const double* aW, const double* aE, const double* aS,
+                        const double* aN, const double* aB, const double* aT,
+                        const double* aP, const double* Su, const double* phi,
+                        double* residual);
+int eaf_residual_3d_f64_device(eaf_cg_t h, const double* aW, const double* aE,
+                               const double* aS, const double* aN, const double* aB,
+                               const double* aT, const double* aP, const double* Su,
+                               const double* phi, double* residual);
+
 /* Bound on every device-side barrier wait, in milliseconds (default 2000). */
 int eaf_cg_set_timeout_ms(eaf_cg_t h, double ms);
 
@@ -284,6 +319,14 @@ int eaf_selftest_barrier_timeout(int device, double timeout_ms);
  * a counter barrier with three memory-ordering variants) or 3 (warp 0
  * exchanges while the other warps wait once on a named barrier; the form
  * the solvers use). All forms fold in the same order. */
+/* Diagnostics (no reference counterpart): checks, on n generated operand
+ * pairs (random over a wide exponent range, exact and near-halfway
+ * quotients, zeros, infinities, NaN), that the division the TDMA sweeps use
+ * (q = t*y refined by one FMA correction from y = 1/m) returns the same
+ * bits as the IEEE division `/`; mismatches must be 0. */
+int eaf_diag_div_check(int device, long long n, unsigned long long seed,
+                       long long* mismatches, long long* fast_path);
+
 int eaf_diag_allreduce_us(int device, int blocks, int threads, int iters,
                           int form, double* us_per_allreduce);
 

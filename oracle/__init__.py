@@ -47,6 +47,10 @@ def lib():
         L.eaf_oracle_matvec.restype = None
         L.eaf_oracle_theta_wrap.argtypes = [ci, ci, ci, _dp]
         L.eaf_oracle_theta_wrap.restype = None
+        L.eaf_oracle_tdma_3d.argtypes = [ci, ci, ci] + [_dp] * 9 + [ci]
+        L.eaf_oracle_tdma_3d.restype = ci
+        L.eaf_oracle_residual_3d.argtypes = [ci, ci, ci] + [_dp] * 9 + [ci, ci]
+        L.eaf_oracle_residual_3d.restype = cd
         L.eaf_oracle_max_threads.argtypes = []
         L.eaf_oracle_max_threads.restype = ci
         _lib = L
@@ -98,6 +102,22 @@ def dot(nr: int, nth: int, nz: int, a: np.ndarray, b: np.ndarray,
 
 def theta_wrap(nr: int, nth: int, nz: int, x: np.ndarray) -> None:
     lib().eaf_oracle_theta_wrap(nr, nth, nz, _p(x))
+
+
+def tdma_3d(system, phi: np.ndarray, n_sweep: int) -> None:
+    """Serial tdma_3d_mpi (src/mod_solver_3d.f90:252-366) in place on phi."""
+    args = [system.nr, system.nth, system.nz] + [_p(a) for a in system.arrays()]
+    rc = lib().eaf_oracle_tdma_3d(*args, _p(phi), int(n_sweep))
+    if rc != 0:
+        raise RuntimeError(f"oracle tdma failed with status {rc}")
+
+
+def residual_3d(system, phi: np.ndarray, plan: tuple | None = None) -> float:
+    """compute_residual_3d_mpi (src/mod_solver_3d.f90:625-694), serial;
+    ``plan=(G, B)`` associates the two sums as the CUDA kernel does."""
+    G, B = plan if plan is not None else (0, 0)
+    args = [system.nr, system.nth, system.nz] + [_p(a) for a in system.arrays()]
+    return lib().eaf_oracle_residual_3d(*args, _p(phi), int(G), int(B))
 
 
 def max_threads() -> int:

@@ -32,6 +32,12 @@
  * `max(x, SMALL)` is written `x > SMALL ? x : SMALL`, the same expression the
  * CUDA kernels use (a NaN x selects SMALL in both).
  *
+ * The same file restates two more routines of that module, serial branch:
+ *   - tdma_3d_mpi, line-by-line TDMA sweeps ......... src/mod_solver_3d.f90:252-366
+ *     with the 1D Thomas solve `tdma` .............. src/mod_solver_3d.f90:22-46
+ *   - compute_residual_3d_mpi ....................... src/mod_solver_3d.f90:625-694
+ * (see eaf_oracle_tdma_3d and eaf_oracle_residual_3d below).
+ *
  * PARITY UNPINNED: the reference is Fortran + MPI and no Fortran compiler or
  * MPI exists where this is built or run, and the reference's tests pin only
  * whole-simulator outcomes, never cg_3d_mpi's iterates. This restatement is
@@ -392,4 +398,204 @@ int eaf_oracle_max_threads(void) {
 #else
     return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------
+ * Line-by-line TDMA, serial branch of tdma_3d_mpi (src/mod_solver_3d.f90:
+ * 252-366). Per sweep: theta-halo refresh (mpi_exchange_halos_3d with one
+ * rank is the periodic copy, src/mod_mpi_topology.f90:303-311), then r
+ * lines for k = 1..nz, j = 1..nth; refresh; theta lines for k, i; refresh;
+ * z lines for j, i. Every line solve reads the current phi in place, so a
+ * line sees the new values of the lines solved before it in that order
+ * (Gauss-Seidel between lines) and the halo values of the last refresh. The
+ * right-hand sides keep the reference's statement and operand order; the
+ * segment endpoints add the lagged halo couplings after the loop.
+ * ---------------------------------------------------------------------- */
+
+/* `tdma` (src/mod_solver_3d.f90:22-46): `sign(SMALL, v)` is copysign (the
+ * sign of a negative zero is kept, as gfortran does). */
+static void thomas(const double* a, const double* b, const double* c,
+                   const double* d, double* x, int n, double* cp, double* dp) {
+    double b1 = b[0];
+    if (fabs(b1) < SMALL) b1 = copysign(SMALL, b1);
+    cp[0] = c[0] / b1;
+    dp[0] = d[0] / b1;
+    for (int i = 1; i < n; ++i) {
+        double m = b[i] - a[i] * cp[i - 1];
+        if (fabs(m) < SMALL) m = copysign(SMALL, m);
+        cp[i] = c[i] / m;
+        dp[i] = (d[i] - a[i] * dp[i - 1]) / m;
+    }
+    x[n - 1] = dp[n - 1];
+    for (int i = n - 2; i >= 0; --i) x[i] = dp[i] - cp[i] * x[i + 1];
+}
+
+int eaf_oracle_tdma_3d(int nr, int nth, int nz, const double* aW, const double* aE,
+                       const double* aS, const double* aN, const double* aB,
+                       const double* aT, const double* aP, const double* Su,
+                       double* phi, int n_sweep) {
+    if (nr < 1 || nth < 1 || nz < 1) return 2;
+    const dims_t D = mkdims(nr, nth, nz);
+    const dims_t* d = &D;
+    int nmax = nr > nth ? nr : nth;
+    if (nz > nmax) nmax = nz;
+    double* buf = (double*)malloc(sizeof(double) * 7 * (size_t)nmax);
+    if (!buf) return 6;
+    double *a = buf, *b = a + nmax, *c = b + nmax, *dd = c + nmax, *x = dd + nmax,
+           *cp = x + nmax, *dp = cp + nmax;
+    for (int sweep = 1; sweep <= n_sweep; ++sweep) {
+        eaf_oracle_theta_wrap(nr, nth, nz, phi);
+        for (int k = 1; k <= nz; ++k)          /* r lines (:286-308) */
+            for (int j = 1; j <= nth; ++j) {
+                for (int i = 1; i <= nr; ++i) {
+                    size_t q = at(d, i, j, k);
+                    a[i - 1] = -aW[q];
+                    b[i - 1] = aP[q];
+                    c[i - 1] = -aE[q];
+                    double t = Su[q] + aS[q] * phi[at(d, i, j - 1, k)] +
+                               aN[q] * phi[at(d, i, j + 1, k)];
+                    dd[i - 1] = t + aB[q] * phi[at(d, i, j, k - 1)] +
+                                aT[q] * phi[at(d, i, j, k + 1)];
+                }
+                dd[0] = dd[0] + aW[at(d, 1, j, k)] * phi[at(d, 0, j, k)];
+                dd[nr - 1] = dd[nr - 1] + aE[at(d, nr, j, k)] * phi[at(d, nr + 1, j, k)];
+                thomas(a, b, c, dd, x, nr, cp, dp);
+                for (int i = 1; i <= nr; ++i) phi[at(d, i, j, k)] = x[i - 1];
+            }
+        eaf_oracle_theta_wrap(nr, nth, nz, phi);
+        for (int k = 1; k <= nz; ++k)          /* theta lines (:311-332) */
+            for (int i = 1; i <= nr; ++i) {
+                for (int j = 1; j <= nth; ++j) {
+                    size_t q = at(d, i, j, k);
+                    a[j - 1] = -aS[q];
+                    b[j - 1] = aP[q];
+                    c[j - 1] = -aN[q];
+                    double t = Su[q];
+                    t = t + aW[q] * phi[at(d, i - 1, j, k)] + aE[q] * phi[at(d, i + 1, j, k)];
+                    dd[j - 1] = t + aB[q] * phi[at(d, i, j, k - 1)] +
+                                aT[q] * phi[at(d, i, j, k + 1)];
+                }
+                dd[0] = dd[0] + aS[at(d, i, 1, k)] * phi[at(d, i, 0, k)];
+                dd[nth - 1] = dd[nth - 1] + aN[at(d, i, nth, k)] * phi[at(d, i, nth + 1, k)];
+                thomas(a, b, c, dd, x, nth, cp, dp);
+                for (int j = 1; j <= nth; ++j) phi[at(d, i, j, k)] = x[j - 1];
+            }
+        eaf_oracle_theta_wrap(nr, nth, nz, phi);
+        for (int j = 1; j <= nth; ++j)         /* z lines (:335-359) */
+            for (int i = 1; i <= nr; ++i) {
+                for (int k = 1; k <= nz; ++k) {
+                    size_t q = at(d, i, j, k);
+                    a[k - 1] = -aB[q];
+                    b[k - 1] = aP[q];
+                    c[k - 1] = -aT[q];
+                    double t = Su[q] + aS[q] * phi[at(d, i, j - 1, k)] +
+                               aN[q] * phi[at(d, i, j + 1, k)];
+                    dd[k - 1] = t + aW[q] * phi[at(d, i - 1, j, k)] +
+                                aE[q] * phi[at(d, i + 1, j, k)];
+                }
+                dd[0] = dd[0] + aB[at(d, i, j, 1)] * phi[at(d, i, j, 0)];
+                dd[nz - 1] = dd[nz - 1] + aT[at(d, i, j, nz)] * phi[at(d, i, j, nz + 1)];
+                thomas(a, b, c, dd, x, nz, cp, dp);
+                for (int k = 1; k <= nz; ++k) phi[at(d, i, j, k)] = x[k - 1];
+            }
+    }
+    free(buf);
+    return 0;
+}
+
+/* compute_residual_3d_mpi (src/mod_solver_3d.f90:625-694), serial: cells
+ * whose row is the identity (aP == 1, all links 0) are skipped; r_local and
+ * the normalisation term keep the reference's operand order; `x**2` is x*x.
+ * G == 0 sums sequentially (k, j, i) as the reference; G > 0 associates the
+ * two sums as the CUDA kernel launched with G blocks of B threads does (the
+ * plan of the CG dots; a skipped cell adds +0.0 there, which leaves a sum
+ * of squares unchanged). */
+static void residual_terms(const dims_t* d, const double* aW, const double* aE,
+                           const double* aS, const double* aN, const double* aB,
+                           const double* aT, const double* aP, const double* Su,
+                           const double* phi, size_t q, double* rr, double* bb) {
+    if (aP[q] == 1.0 && aW[q] == 0.0 && aE[q] == 0.0 && aS[q] == 0.0 && aN[q] == 0.0 &&
+        aB[q] == 0.0 && aT[q] == 0.0) {
+        *rr = 0.0;
+        *bb = 0.0;
+        return;
+    }
+    double r = Su[q] - aP[q] * phi[q] + aS[q] * phi[q - d->sx] + aN[q] * phi[q + d->sx];
+    r = r + aW[q] * phi[q - 1] + aE[q] * phi[q + 1];
+    r = r + aB[q] * phi[q - d->sxy] + aT[q] * phi[q + d->sxy];
+    double t = fabs(Su[q]) + fabs(aP[q] * phi[q]) + SMALL;
+    *rr = r * r;
+    *bb = t * t;
+}
+
+double eaf_oracle_residual_3d(int nr, int nth, int nz, const double* aW, const double* aE,
+                              const double* aS, const double* aN, const double* aB,
+                              const double* aT, const double* aP, const double* Su,
+                              const double* phi, int G, int B) {
+    const dims_t D = mkdims(nr, nth, nz);
+    const dims_t* d = &D;
+    double sum_r = 0.0, sum_b = 0.0;
+    if (G <= 0) {
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= nth; ++j)
+                for (int i = 1; i <= nr; ++i) {
+                    size_t q = at(d, i, j, k);
+                    if (aP[q] == 1.0 && aW[q] == 0.0 && aE[q] == 0.0 && aS[q] == 0.0 &&
+                        aN[q] == 0.0 && aB[q] == 0.0 && aT[q] == 0.0)
+                        continue;
+                    double rr, bb;
+                    residual_terms(d, aW, aE, aS, aN, aB, aT, aP, Su, phi, q, &rr, &bb);
+                    sum_r = sum_r + rr;
+                    sum_b = sum_b + bb;
+                }
+    } else {
+        const int n = nr * nth * nz;
+        const int chunk = (n + G - 1) / G;
+        double* lane_r = (double*)malloc(sizeof(double) * (size_t)B * 2);
+        double* part = (double*)malloc(sizeof(double) * (size_t)G * 2);
+        if (!lane_r || !part) {
+            free(lane_r);
+            free(part);
+            return NAN;
+        }
+        double* lane_b = lane_r + B;
+        for (int g = 0; g < G; ++g) {
+            int begin = g * chunk < n ? g * chunk : n;
+            int end = begin + chunk < n ? begin + chunk : n;
+            for (int t = 0; t < B; ++t) {
+                double sr = 0.0, sb = 0.0;
+                for (int c = begin + t; c < end; c += B) {
+                    double rr, bb;
+                    residual_terms(d, aW, aE, aS, aN, aB, aT, aP, Su, phi,
+                                   compact_to_halo(d, c), &rr, &bb);
+                    sr = sr + rr;
+                    sb = sb + bb;
+                }
+                lane_r[t] = sr;
+                lane_b[t] = sb;
+            }
+            part[g] = block_tree(lane_r, B);
+            part[G + g] = block_tree(lane_b, B);
+        }
+        for (int m = 0; m < 2; ++m) {
+            const double* pm = part + (size_t)m * G;
+            double tot;
+            if (G == 1) {
+                tot = pm[0];
+            } else {
+                double v[32];
+                for (int l = 0; l < 32; ++l) {
+                    double s = 0.0;
+                    for (int g = l; g < G; g += 32) s = s + pm[g];
+                    v[l] = s;
+                }
+                butterfly32(v);
+                tot = v[0];
+            }
+            if (m == 0) sum_r = tot; else sum_b = tot;
+        }
+        free(lane_r);
+        free(part);
+    }
+    return sqrt(sum_r) / (sqrt(sum_b) + SMALL);
 }
