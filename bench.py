@@ -418,6 +418,78 @@ def run_fine(args):
     return 0
 
 
+def run_tdma(args):
+    """Line-by-line TDMA (tdma_3d_mpi) on a 60x120x84 transport system:
+    args.tdma_sweeps sweeps per step from phi = 0, device-resident inputs
+    (value) and through the host-pointer entry (e2e: 9 uploads + 1 download
+    per step), with the single-thread CPU restatement as baseline (the
+    reference's serial sweeps are one sequential loop nest)."""
+    import numpy as np
+    import torch
+    eaf = importlib.import_module(PKG)
+    g = importlib.import_module(PKG + ".eafgen")
+    nr, nth, nz = MESH[:3]
+    n = nr * nth * nz
+    ns = args.tdma_sweeps
+    s = g.make_transport_system(nr, nth, nz, seed=0)
+    dev = [torch.from_numpy(a).cuda() for a in s.arrays()]
+    phi = torch.zeros(g.halo_shape(nr, nth, nz), dtype=torch.float64, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    host = [eaf.host_empty(g.halo_shape(nr, nth, nz)) for _ in range(9)]
+    for h, a in zip(host, s.arrays()):
+        h[...] = a
+    with eaf.CGSolver(nr, nth, nz) as cg:
+        for _ in range(args.warmup):
+            phi.zero_()
+            cg.tdma(dev, phi, ns, device_ptrs=True)
+        ms = kms = 0.0
+        for _ in range(args.steps):
+            phi.zero_()
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            cg.tdma(dev, phi, ns, device_ptrs=True)
+            t = cg.last_timing()
+            ms += t["solve_ms"]
+            kms += t["kernel_ms"]
+        e2e = 0.0
+        for _ in range(args.steps):
+            host[8][...] = 0.0
+            cg.tdma(host[:8], host[8], ns)
+            e2e += cg.last_timing()["e2e_ms"]
+        x_gpu = host[8].copy()
+        launch = cg.last_launch()
+    # CPU baseline: the oracle's serial sweeps on one thread, same system.
+    import oracle
+    x_cpu = g.zeros_phi(nr, nth, nz)
+    t0 = time.perf_counter()
+    oracle.tdma_3d(s, x_cpu, ns)
+    cpu_s = time.perf_counter() - t0
+    crit = sum((A + B - 1) * L for A, B, L in ((nth, nz, nr), (nr, nz, nth), (nth, nr, nz)))
+    value = n * ns * args.steps / (ms / 1e3)
+    line = _base_line("line-TDMA cell-sweeps/s (60x120x84 transport system)", value,
+                      "cell-sweeps/s", args.steps, args.warmup, ms / args.steps,
+                      f"tdma_3d_mpi, {ns} sweeps from phi = 0",
+                      {"mesh": [nr, nth, nz], "cells": n, "sweeps_per_step": ns,
+                       "launch": {"grid": launch[0], "block": launch[1]},
+                       "l2": "flushed between steps (256 MiB memset)"})
+    line["e2e"] = {"value": n * ns * args.steps / (e2e / 1e3), "unit": "cell-sweeps/s",
+                   "h2d_bytes_per_step": 9 * host[0].nbytes,
+                   "d2h_bytes_per_step": host[0].nbytes}
+    line["bitwise_equal_to_cpu"] = bool(np.array_equal(x_gpu, x_cpu))
+    line["cpu_baseline"] = {"value": n * ns / cpu_s, "unit": "cell-sweeps/s", "cores": 1,
+                            "kind": "port",
+                            "sample": f"oracle port of tdma_3d_mpi, {ns} sweeps, one "
+                                      f"thread, {cpu_s:.2f} s"}
+    line["critical_path"] = {
+        "elements_per_sweep": crit,
+        "ns_per_element": 1e6 * (kms / args.steps) / ns / crit,
+        "note": "lines of one direction run as a wavefront: (A+B-1) dependent line "
+                "solves of L elements each, one sequential Thomas step per element"}
+    line["gpu_launches"] = 2 * args.steps
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch(args):
     """96 uneven systems (40 at 12x24x16, 30 at 18x36x24, 20 at 35x70x50,
     6 at 60x120x84; seed = system id) in one persistent launch replayed from
@@ -547,7 +619,8 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-iters", type=int, default=1500,
                     help="iteration cap per reference-arm step (bounded sample)")
-    ap.add_argument("--workload", choices=["production", "fine", "batch", "serve"],
+    ap.add_argument("--tdma-sweeps", type=int, default=3)
+    ap.add_argument("--workload", choices=["production", "fine", "batch", "serve", "tdma"],
                     default="production")
     ap.add_argument("--mixed-outer", type=int, default=30)
     ap.add_argument("--mixed-inner", type=int, default=3000)
@@ -557,7 +630,8 @@ def main(argv=None):
     ap.add_argument("--serve-mixed", action="store_true")
     args = ap.parse_args(argv)
     if args.workload != "production" and args.impl == "ours":
-        return {"fine": run_fine, "batch": run_batch, "serve": run_serve}[args.workload](args)
+        return {"fine": run_fine, "batch": run_batch, "serve": run_serve,
+                "tdma": run_tdma}[args.workload](args)
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local_rank = _env_int("LOCAL_RANK", 0)

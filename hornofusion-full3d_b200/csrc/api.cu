@@ -46,7 +46,7 @@ struct eaf_cg {
   double last_solve_ms, last_kernel_ms, last_e2e_ms;
   int last_sym, last_kernels;
   int last_grid, last_block;
-  int* tdma_prog;    // per-owner progress of the TDMA sweeps (lazy)
+  double* tdma_mbox;  // TDMA line hand-over slots (lazy)
   double* tdma_fac;  // TDMA line factors (lazy)
 };
 
@@ -97,7 +97,7 @@ static void free_handle(eaf_cg* h) {
   cudaFree(h->ws.counter);
   cudaFree(h->ws.err);
   cudaFree(h->ws.result);
-  cudaFree(h->tdma_prog);
+  cudaFree(h->tdma_mbox);
   cudaFree(h->tdma_fac);
   if (h->res_h) cudaFreeHost(h->res_h);
   for (int i = 0; i < 6; ++i)
@@ -422,8 +422,9 @@ int solve_host(eaf_cg* h, const double* const arr[8], double* phi, const SolveOp
 // Line-by-line TDMA sweeps and the transport residual on the handle's mesh.
 // ---------------------------------------------------------------------------
 int enqueue_tdma(eaf_cg* h, const HaloInputs& in, double* phi, int n_sweep) {
-  if (!h->tdma_prog) {
-    EAF_CUDA(cudaMalloc((void**)&h->tdma_prog, sizeof(int) * eaf::tdma_progress_ints()));
+  if (!h->tdma_mbox) {
+    EAF_CUDA(cudaMalloc((void**)&h->tdma_mbox,
+                        sizeof(double) * eaf::tdma_mailbox_doubles(h->nr, h->nth, h->nz)));
   }
   if (!h->tdma_fac) {
     EAF_CUDA(cudaMalloc((void**)&h->tdma_fac,
@@ -434,7 +435,7 @@ int enqueue_tdma(eaf_cg* h, const HaloInputs& in, double* phi, int n_sweep) {
   EAF_CUDA(cudaEventRecord(h->ev[1], h->st));
   EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
   if (n_sweep > 0) {
-    EAF_CUDA(eaf::launch_tdma_f64(in, phi, h->nr, h->nth, h->nz, n_sweep, h->tdma_prog,
+    EAF_CUDA(eaf::launch_tdma_f64(in, phi, h->nr, h->nth, h->nz, n_sweep, h->tdma_mbox,
                                   h->tdma_fac, h->ws, h->timeout_ns, h->st));
   }
   EAF_CUDA(cudaEventRecord(h->ev[3], h->st));

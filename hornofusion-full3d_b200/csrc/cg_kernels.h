@@ -125,15 +125,16 @@ cudaError_t launch_batch_mixed(const BatchTables& t, int grid, int block,
                                double inner_tol, uint64_t timeout_ns, cudaStream_t st);
 const void* batch_f64_kernel_ptr();
 // Line-by-line TDMA sweeps (tdma_3d_mpi, serial) on halo-layout arrays, in
-// place on phi; `prog` holds tdma_progress_ints() ints of per-owner
-// progress. One cooperative launch of tdma_grid() warps.
+// place on phi; `mbox` holds tdma_mailbox_doubles() doubles of line
+// hand-over slots. One cooperative launch of tdma_grid() warps; every mesh
+// extent at most 1024.
 // `fac` holds tdma_factor_doubles() doubles of line factors (computed by the
 // launch from the coefficients).
-size_t tdma_progress_ints();
+size_t tdma_mailbox_doubles(int nr, int nth, int nz);
 size_t tdma_factor_doubles(int nr, int nth, int nz);
 int tdma_grid(int nr, int nth, int nz);
 cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, int nz,
-                            int n_sweep, int* prog, double* fac, const GroupWs& ws,
+                            int n_sweep, double* mbox, double* fac, const GroupWs& ws,
                             uint64_t timeout_ns, cudaStream_t st);
 const void* tdma_kernel_ptr();
 // compute_residual_3d_mpi (serial) into ws.result->residual.

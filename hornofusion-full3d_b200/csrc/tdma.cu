@@ -13,8 +13,13 @@
 // (a, b-1) only. One warp owns one index of the grid and solves its chain of
 // lines in order: the in-chain dependency is the warp's own previous line,
 // kept in shared memory; the cross-chain one is the neighbouring owner's
-// line, published through a per-owner progress counter (release/acquire,
-// bounded wait). Owners are chosen so that the cross-chain value is the
+// line, which the owner also writes into a mailbox -- one slot per cell,
+// marked empty with a signalling NaN that arithmetic never produces -- and
+// the consumer polls the values themselves (bounded wait): one L2 round trip
+// per hand-over and no fence, since the data is the signal. The consumer
+// marks the slots empty again; slots alternate by sweep parity, and the
+// grid barrier between directions orders a reset before the slot's next
+// use. Owners are chosen so that the cross-chain value is the
 // THIRD term of the reference's right-hand side
 //   d = (Su + c1m*p1m) + c1p*p1p;  d = (d + c2m*p2m) + c2p*p2p
 // (p1m the in-chain neighbour, p2m the cross-chain one): everything before
@@ -43,7 +48,7 @@ struct TdmaArgs {
   long long sx, sxy;  // halo strides of j and k
   int n_sweep;
   int lmax;
-  int* prog;          // per-owner progress, [3 directions][kTdmaMaxOwners]
+  double* mbox;       // hand-over slots, [2 parities][3 directions][n cells]
   double* fac;        // line factors, [3 directions][m, y, cp][n cells]
   GroupWs ws;
   uint64_t timeout_ns;
@@ -90,25 +95,6 @@ __device__ __forceinline__ double sign_small(double v) {
   return fabs(v) < kSmall ? copysign(kSmall, v) : v;
 }
 
-// Waits (lane 0) until *p >= target; false on timeout or a group error.
-__device__ bool wait_progress(const int* p, int target, const TdmaArgs& a) {
-  uint64_t t0 = 0;
-  uint32_t spins = 0;
-  for (;;) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    if (v >= target) return true;
-    if ((++spins & 63u) == 0) {
-      if (spins == 64u) t0 = global_ns();
-      if (ld_volatile_i32(a.ws.err) != 0) return false;
-      if (global_ns() - t0 > a.timeout_ns) {
-        atomicCAS(a.ws.err, 0, (int)EAF_ETIMEOUT);
-        return false;
-      }
-    }
-  }
-}
-
 // Serial theta-periodic halo copy (src/mod_mpi_topology.f90:303-311) over
 // all (i, k) columns of the halo layout, each column's four copies in the
 // reference's statement order.
@@ -130,7 +116,7 @@ __device__ void theta_wrap(const TdmaArgs& a) {
   }
 }
 
-constexpr int kTdmaMaxOwners = 4096;
+constexpr int kTdmaMaxLine = 1024;  // 32 elements per lane in a hand-over mask
 
 // ---------------------------------------------------------------------------
 // Correctly rounded t / m from a precomputed y = RN(1/m), by one correction
@@ -143,16 +129,21 @@ constexpr int kTdmaMaxOwners = 4096;
 // -- zeros, subnormals, huge values, infinities, NaN -- takes `/` itself. The
 // point is latency: the reciprocal leaves the sweep's dependent chain.
 // ---------------------------------------------------------------------------
+// Empty hand-over slot: a signalling NaN (IEEE arithmetic only delivers
+// quiet NaNs, so no solution value has this pattern).
+#define kEmptySlot __longlong_as_double(0x7ff000017ff00001ll)
+constexpr unsigned long long kEmptyBits = 0x7ff000017ff00001ull;
+
 __device__ __forceinline__ bool exp_in_safe_range(double v) {
   const unsigned e = (unsigned)((unsigned long long)__double_as_longlong(v) >> 52) & 0x7ffu;
   return e - 523u <= 1000u;  // biased exponent 523..1523
 }
 
 __device__ __forceinline__ double div_by_recip(double t, double m, double y, bool m_ok) {
-  if (m_ok && exp_in_safe_range(t)) {
+  if (m_ok && (t == 0.0 || exp_in_safe_range(t))) {
     const double q = t * y;
-    const double r = __fma_rn(-q, m, t);
-    return __fma_rn(r, y, q);
+    const double c = __fma_rn(__fma_rn(-q, m, t), y, q);
+    return t == 0.0 ? q : c;
   }
   return t / m;
 }
@@ -189,6 +180,9 @@ __global__ void tdma_factor_kernel(TdmaArgs a) {
       M[e] = m;
       Y[e] = exp_in_safe_range(m) ? 1.0 / m : 0.0;
       CP[e] = cp;
+      const long long slot = (long long)dir * n + line * d.L + e;
+      a.mbox[slot] = kEmptySlot;
+      a.mbox[3 * n + slot] = kEmptySlot;
     }
   }
 }
@@ -238,12 +232,34 @@ __device__ __forceinline__ void thomas_line(const LineSmem& s, int L) {
   const double* __restrict__ rhs = s.rhs;
   double* __restrict__ dpa = s.dp;
   double* __restrict__ x = s.x;
-  double dp = div_by_recip(rhs[0], mm[0], yy[0], yy[0] != 0.0);
+  // Forward pass on the correction path only, with the range conditions
+  // OR-ed off the dependent chain; a line with any operand outside the safe
+  // range (rare) is redone with `/` throughout. A zero numerator is exact on
+  // this path as q = t*y itself (the correction would turn -0 into +0).
+  bool ok = yy[0] != 0.0 && (rhs[0] == 0.0 || exp_in_safe_range(rhs[0]));
+  double dp;
+  {
+    const double t = rhs[0], q = t * yy[0];
+    const double c = __fma_rn(__fma_rn(-q, mm[0], t), yy[0], q);
+    dp = t == 0.0 ? q : c;
+  }
   dpa[0] = dp;
   for (int i = 1; i < L; ++i) {
-    const double y = yy[i];
-    dp = div_by_recip(rhs[i] - lo[i] * dp, mm[i], y, y != 0.0);
+    const double y = yy[i], m = mm[i];
+    const double t = rhs[i] - lo[i] * dp;
+    ok = ok & (y != 0.0) & (t == 0.0 || exp_in_safe_range(t));
+    const double q = t * y;
+    const double c = __fma_rn(__fma_rn(-q, m, t), y, q);
+    dp = t == 0.0 ? q : c;
     dpa[i] = dp;
+  }
+  if (!ok) {
+    dp = rhs[0] / mm[0];
+    dpa[0] = dp;
+    for (int i = 1; i < L; ++i) {
+      dp = (rhs[i] - lo[i] * dp) / mm[i];
+      dpa[i] = dp;
+    }
   }
   double xv = dp;
   x[L - 1] = xv;
@@ -285,26 +301,60 @@ __global__ void __launch_bounds__(32) tdma_kernel(TdmaArgs a) {
       theta_wrap(a);
       if (!(ok = group_barrier<1>(g))) break;
       const Dir d = make_dir(a, dir);
-      int* prog = a.prog + dir * kTdmaMaxOwners;
-      const int stamp0 = (sweep - 1) * d.A;  // progress before this sweep
       const long long ncell = (long long)a.nr * a.nth * a.nz;
       const double* fdir = a.fac + (long long)dir * 3 * ncell;
+      double* mb = a.mbox + ((long long)(sweep & 1) * 3 + dir) * ncell;
       for (int b = blockIdx.x; b < d.B && ok; b += gridDim.x) {
         const long long qb = base + b * d.sb;
-        const double* fb = fdir + (long long)b * d.A * d.L;  // line (0, b)
+        const long long lines_b = (long long)b * d.A * d.L;  // line (0, b)
+        const double* fb = fdir + lines_b;
+        double* mine = mb + lines_b;
+        unsigned long long* from =
+            b > 0 ? reinterpret_cast<unsigned long long*>(mb + lines_b - (long long)d.A * d.L)
+                  : nullptr;
+        const bool feeds = b + 1 < d.B;
         line_phase1(a, d, s, qb, 0, lane, ends, fb);
         for (int ch = 0; ch < d.A; ++ch) {
           const long long q0 = qb + ch * d.sa;
-          // The previous owner's line `ch` must be done.
-          int go = 1;
-          if (lane == 0 && b > 0) go = wait_progress(prog + b - 1, stamp0 + ch + 1, a);
-          go = __shfl_sync(0xffffffffu, go, 0);
-          if (!go) { ok = false; break; }
           __syncwarp();
-          for (int e = lane; e < d.L; e += 32) {
-            const long long q = q0 + e * d.se;
-            const double t = s.rhs[e] + s.c2m[e] * __ldcg(phi + q - d.s2);
-            s.rhs[e] = t + s.c2t[e];
+          if (b == 0) {  // the second pair's minus side is a halo
+            for (int e = lane; e < d.L; e += 32) {
+              const double t = s.rhs[e] + s.c2m[e] * __ldcg(phi + q0 + e * d.se - d.s2);
+              s.rhs[e] = t + s.c2t[e];
+            }
+          } else {  // the previous owner's line `ch`, from its mailbox
+            unsigned long long* slot = from + (long long)ch * d.L;
+            unsigned pend = 0;
+            for (int k = 0; lane + 32 * k < d.L; ++k) pend |= 1u << k;
+            uint64_t t0 = 0;
+            uint32_t spins = 0;
+            for (;;) {
+              for (int k = 0; lane + 32 * k < d.L; ++k) {
+                if (!(pend & (1u << k))) continue;
+                const int e = lane + 32 * k;
+                const unsigned long long v = ld_relaxed_u64(slot + e);
+                if (v == kEmptyBits) continue;
+                const double t = s.rhs[e] + s.c2m[e] * __longlong_as_double((long long)v);
+                s.rhs[e] = t + s.c2t[e];
+                slot[e] = kEmptyBits;
+                pend &= ~(1u << k);
+              }
+              if (!__any_sync(0xffffffffu, pend != 0)) break;
+              if ((++spins & 63u) == 0) {
+                int stop = 0;
+                if (lane == 0) {
+                  if (spins == 64u) t0 = global_ns();
+                  if (ld_volatile_i32(a.ws.err) != 0) {
+                    stop = 1;
+                  } else if (global_ns() - t0 > a.timeout_ns) {
+                    atomicCAS(a.ws.err, 0, (int)EAF_ETIMEOUT);
+                    stop = 1;
+                  }
+                }
+                if (__shfl_sync(0xffffffffu, stop, 0)) break;
+              }
+            }
+            if (__any_sync(0xffffffffu, pend != 0)) { ok = false; break; }
           }
           __syncwarp();
           if (lane == 0) {
@@ -314,18 +364,14 @@ __global__ void __launch_bounds__(32) tdma_kernel(TdmaArgs a) {
             thomas_line(s, d.L);
           }
           __syncwarp();
-          for (int e = lane; e < d.L; e += 32) phi[q0 + e * d.se] = s.x[e];
+          for (int e = lane; e < d.L; e += 32) {
+            const double xv = s.x[e];
+            if (feeds) mine[(long long)ch * d.L + e] = xv;
+            phi[q0 + e * d.se] = xv;
+          }
           __syncwarp();
-          // Next line's loads overlap this line's publish.
           if (ch + 1 < d.A)
             line_phase1(a, d, s, q0 + d.sa, ch + 1, lane, ends, fb + (long long)(ch + 1) * d.L);
-          __threadfence();
-          __syncwarp();
-          if (lane == 0) {
-            asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(prog + b),
-                         "r"(stamp0 + ch + 1)
-                         : "memory");
-          }
         }
       }
     }
@@ -454,7 +500,7 @@ __global__ void div_check_kernel(long long n, unsigned long long seed,
     const bool same = (__double_as_longlong(a) == __double_as_longlong(b)) ||
                       (a != a && b != b);
     bad += same ? 0 : 1;
-    fast += (m_ok && exp_in_safe_range(t)) ? 1 : 0;
+    fast += (m_ok && (t == 0.0 || exp_in_safe_range(t))) ? 1 : 0;
   }
   atomicAdd(counts, bad);
   atomicAdd(counts + 1, fast);
@@ -462,7 +508,9 @@ __global__ void div_check_kernel(long long n, unsigned long long seed,
 
 }  // namespace
 
-size_t tdma_progress_ints() { return (size_t)3 * kTdmaMaxOwners; }
+size_t tdma_mailbox_doubles(int nr, int nth, int nz) {
+  return (size_t)6 * nr * nth * nz;
+}
 
 int tdma_grid(int nr, int nth, int nz) {
   // Owners per direction: k (r lines), k (theta lines), i (z lines).
@@ -474,9 +522,10 @@ size_t tdma_factor_doubles(int nr, int nth, int nz) {
 }
 
 cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, int nz,
-                            int n_sweep, int* prog, double* fac, const GroupWs& ws,
+                            int n_sweep, double* mbox, double* fac, const GroupWs& ws,
                             uint64_t timeout_ns, cudaStream_t st) {
-  if (nz > kTdmaMaxOwners || nr > kTdmaMaxOwners) return cudaErrorInvalidValue;
+  if (nr > kTdmaMaxLine || nth > kTdmaMaxLine || nz > kTdmaMaxLine)
+    return cudaErrorInvalidValue;
   TdmaArgs a;
   a.in = in;
   a.phi = phi;
@@ -489,7 +538,7 @@ cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, 
   int lmax = nr > nth ? nr : nth;
   if (nz > lmax) lmax = nz;
   a.lmax = lmax;
-  a.prog = prog;
+  a.mbox = mbox;
   a.fac = fac;
   a.ws = ws;
   a.timeout_ns = timeout_ns;
@@ -507,8 +556,6 @@ cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, 
     tdma_factor_kernel<<<(unsigned)fg, fb, 0, st>>>(a);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess)
-    e = cudaMemsetAsync(prog, 0, sizeof(int) * tdma_progress_ints(), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
