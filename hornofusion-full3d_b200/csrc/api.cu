@@ -431,7 +431,7 @@ int enqueue_tdma(eaf_cg* h, const HaloInputs& in, double* phi, int n_sweep) {
                         sizeof(double) * eaf::tdma_factor_doubles(h->nr, h->nth, h->nz)));
   }
   h->last_grid = eaf::tdma_grid(h->nr, h->nth, h->nz);
-  h->last_block = 32;
+  h->last_block = 64;
   EAF_CUDA(cudaEventRecord(h->ev[1], h->st));
   EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
   if (n_sweep > 0) {

@@ -187,32 +187,62 @@ __global__ void tdma_factor_kernel(TdmaArgs a) {
   }
 }
 
-// Shared memory of one warp: nine line arrays of lmax doubles.
-struct LineSmem {
-  double *lo, *m, *y, *cp, *rhs, *c2m, *c2t, *dp, *x;
+// ---------------------------------------------------------------------------
+// Per owner, two warps: the LOADER fetches line ch+1 (coefficients, factors,
+// the old neighbour values it needs, the end couplings) into one of two
+// shared-memory buffers while the SOLVER finishes line ch; the solver then
+// only forms the right-hand side from shared memory plus the two new values
+// (its own previous line, the previous owner's mailbox) and runs the Thomas
+// recurrences. Hand-shake: named barriers FULL_k / EMPTY_k per buffer k (a
+// producer never arrives twice on one barrier before its consumer synced).
+// ---------------------------------------------------------------------------
+constexpr int kBarFull0 = 3, kBarEmpty0 = 5;  // FULL_k = 3 + k, EMPTY_k = 5 + k
+constexpr int kTdmaBlock = 64;
+constexpr int kBufArrays = 11;
+
+struct LineBuf {
+  double *su, *c1m, *c1t, *c2m, *c2t, *p1h, *p2h, *lo, *m, *y, *cp;
 };
 
-// Phase 1 of line `ch` of owner `b` (no wait needed): everything of the
-// right-hand side before the cross-owner term, the second pair's
-// coefficient and plus-side term, the tridiagonal coefficients, and the
-// two lagged end couplings (halo values, constant during a sweep) as
-// products, added in order after the full right-hand side.
-__device__ __forceinline__ void line_phase1(const TdmaArgs& a, const Dir& d,
-                                            const LineSmem& s, long long q0, int ch,
-                                            int lane, double* ends, const double* fm) {
+__device__ __forceinline__ LineBuf line_buf(double* base, int lmax) {
+  LineBuf b;
+  b.su = base;
+  b.c1m = b.su + lmax;
+  b.c1t = b.c1m + lmax;
+  b.c2m = b.c1t + lmax;
+  b.c2t = b.c2m + lmax;
+  b.p1h = b.c2t + lmax;
+  b.p2h = b.p1h + lmax;
+  b.lo = b.p2h + lmax;
+  b.m = b.lo + lmax;
+  b.y = b.m + lmax;
+  b.cp = b.y + lmax;
+  return b;
+}
+
+// Loader: everything of line `ch` of owner `b` that does not depend on this
+// sweep's new values. Products are formed as the reference forms them
+// (c1p*p1p and c2p*p2p are added as whole terms); halo values for the
+// first line of the chain (p1) and for owner 0 (p2).
+__device__ __forceinline__ void load_line(const TdmaArgs& a, const Dir& d, const LineBuf& lb,
+                                          double* ends, long long q0, int ch, int b,
+                                          const double* fm, int lane) {
   const double* __restrict__ phi = a.phi;
   const double* __restrict__ Su = a.in.Su;
   const long long n = (long long)a.nr * a.nth * a.nz;
   for (int e = lane; e < d.L; e += 32) {
     const long long q = q0 + e * d.se;
-    const double p1m = ch > 0 ? s.x[e] : __ldcg(phi + q - d.s1);
-    s.rhs[e] = Su[q] + d.c1m[q] * p1m + d.c1p[q] * __ldcg(phi + q + d.s1);
-    s.c2m[e] = d.c2m[q];
-    s.c2t[e] = d.c2p[q] * __ldcg(phi + q + d.s2);
-    s.lo[e] = -d.lm[q];
-    s.m[e] = __ldcg(fm + e);
-    s.y[e] = __ldcg(fm + n + e);
-    s.cp[e] = __ldcg(fm + 2 * n + e);
+    lb.su[e] = Su[q];
+    lb.c1m[e] = d.c1m[q];
+    lb.c1t[e] = d.c1p[q] * __ldcg(phi + q + d.s1);
+    lb.c2m[e] = d.c2m[q];
+    lb.c2t[e] = d.c2p[q] * __ldcg(phi + q + d.s2);
+    if (ch == 0) lb.p1h[e] = __ldcg(phi + q - d.s1);
+    if (b == 0) lb.p2h[e] = __ldcg(phi + q - d.s2);
+    lb.lo[e] = -d.lm[q];
+    lb.m[e] = __ldcg(fm + e);
+    lb.y[e] = __ldcg(fm + n + e);
+    lb.cp[e] = __ldcg(fm + 2 * n + e);
   }
   if (lane == 0) {
     const long long qL = q0 + (long long)(d.L - 1) * d.se;
@@ -221,21 +251,19 @@ __device__ __forceinline__ void line_phase1(const TdmaArgs& a, const Dir& d,
   }
 }
 
-// The phi-dependent half of tdma (src/mod_solver_3d.f90:32-45) of one line,
-// lane 0: dp_1 = d_1 / m_1, dp_i = (d_i - a_i dp_{i-1}) / m_i, then the back
-// substitution x_i = dp_i - cp_i x_{i+1}, into s.x.
-__device__ __forceinline__ void thomas_line(const LineSmem& s, int L) {
-  const double* __restrict__ lo = s.lo;
-  const double* __restrict__ mm = s.m;
-  const double* __restrict__ yy = s.y;
-  const double* __restrict__ cpa = s.cp;
-  const double* __restrict__ rhs = s.rhs;
-  double* __restrict__ dpa = s.dp;
-  double* __restrict__ x = s.x;
-  // Forward pass on the correction path only, with the range conditions
-  // OR-ed off the dependent chain; a line with any operand outside the safe
-  // range (rare) is redone with `/` throughout. A zero numerator is exact on
-  // this path as q = t*y itself (the correction would turn -0 into +0).
+// The phi-dependent half of tdma (src/mod_solver_3d.f90:32-45), lane 0:
+// dp_1 = d_1 / m_1, dp_i = (d_i - a_i dp_{i-1}) / m_i, x_i = dp_i - cp_i x_{i+1}.
+// The forward pass runs on the correction path only, its range conditions
+// OR-ed off the dependent chain; a line with any operand outside the safe
+// range (rare) is redone with `/` throughout. A zero numerator is exact on
+// this path as q = t*y itself (the correction would turn -0 into +0).
+__device__ __forceinline__ void thomas_line(const LineBuf& lb, const double* __restrict__ rhs,
+                                            double* __restrict__ dpa,
+                                            double* __restrict__ x, int L) {
+  const double* __restrict__ lo = lb.lo;
+  const double* __restrict__ mm = lb.m;
+  const double* __restrict__ yy = lb.y;
+  const double* __restrict__ cpa = lb.cp;
   bool ok = yy[0] != 0.0 && (rhs[0] == 0.0 || exp_in_safe_range(rhs[0]));
   double dp;
   {
@@ -269,20 +297,53 @@ __device__ __forceinline__ void thomas_line(const LineSmem& s, int L) {
   }
 }
 
-__global__ void __launch_bounds__(32) tdma_kernel(TdmaArgs a) {
+// Polls the previous owner's mailbox for line values (bounded); completes
+// rhs_e = (rhs_e + c2m_e * p2m_e) + c2t_e as they arrive and empties the
+// slots. False if the wait gave up.
+__device__ bool take_mailbox(const TdmaArgs& a, unsigned long long* slot, const LineBuf& lb,
+                             double* rhs, int L, int lane) {
+  unsigned pend = 0;
+  for (int k = 0; lane + 32 * k < L; ++k) pend |= 1u << k;
+  uint64_t t0 = 0;
+  uint32_t spins = 0;
+  for (;;) {
+    for (int k = 0; lane + 32 * k < L; ++k) {
+      if (!(pend & (1u << k))) continue;
+      const int e = lane + 32 * k;
+      const unsigned long long v = ld_relaxed_u64(slot + e);
+      if (v == kEmptyBits) continue;
+      const double t = rhs[e] + lb.c2m[e] * __longlong_as_double((long long)v);
+      rhs[e] = t + lb.c2t[e];
+      slot[e] = kEmptyBits;
+      pend &= ~(1u << k);
+    }
+    if (!__any_sync(0xffffffffu, pend != 0)) return true;
+    if ((++spins & 63u) == 0) {
+      int stop = 0;
+      if (lane == 0) {
+        if (spins == 64u) t0 = global_ns();
+        if (ld_volatile_i32(a.ws.err) != 0) {
+          stop = 1;
+        } else if (global_ns() - t0 > a.timeout_ns) {
+          atomicCAS(a.ws.err, 0, (int)EAF_ETIMEOUT);
+          stop = 1;
+        }
+      }
+      if (__shfl_sync(0xffffffffu, stop, 0)) return false;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTdmaBlock) tdma_kernel(TdmaArgs a) {
   extern __shared__ __align__(16) double sm[];
-  LineSmem s;
-  s.lo = sm;
-  s.m = s.lo + a.lmax;
-  s.y = s.m + a.lmax;
-  s.cp = s.y + a.lmax;
-  s.rhs = s.cp + a.lmax;
-  s.c2m = s.rhs + a.lmax;
-  s.c2t = s.c2m + a.lmax;
-  s.dp = s.c2t + a.lmax;
-  s.x = s.dp + a.lmax;
-  __shared__ double ends[2];
-  const int lane = threadIdx.x;
+  __shared__ double s_ends[2][2];
+  const LineBuf buf0 = line_buf(sm, a.lmax);
+  const LineBuf buf1 = line_buf(sm + kBufArrays * a.lmax, a.lmax);
+  double* s_x = sm + 2 * kBufArrays * a.lmax;
+  double* s_rhs = s_x + a.lmax;
+  double* s_dp = s_rhs + a.lmax;
+  const int lane = threadIdx.x & 31;
+  const bool loader = threadIdx.x >= 32;
   Group g;
   g.counter = a.ws.counter;
   g.err = a.ws.err;
@@ -304,76 +365,66 @@ __global__ void __launch_bounds__(32) tdma_kernel(TdmaArgs a) {
       const long long ncell = (long long)a.nr * a.nth * a.nz;
       const double* fdir = a.fac + (long long)dir * 3 * ncell;
       double* mb = a.mbox + ((long long)(sweep & 1) * 3 + dir) * ncell;
-      for (int b = blockIdx.x; b < d.B && ok; b += gridDim.x) {
+      for (int b = blockIdx.x; b < d.B; b += gridDim.x) {
         const long long qb = base + b * d.sb;
         const long long lines_b = (long long)b * d.A * d.L;  // line (0, b)
-        const double* fb = fdir + lines_b;
+        if (loader) {
+          for (int ch = 0; ch < d.A; ++ch) {
+            const int k = ch & 1;
+            if (ch >= 2) named_sync(kBarEmpty0 + k, kTdmaBlock);
+            load_line(a, d, k ? buf1 : buf0, s_ends[k], qb + ch * d.sa, ch, b,
+                      fdir + lines_b + (long long)ch * d.L, lane);
+            named_arrive(kBarFull0 + k, kTdmaBlock);
+          }
+          continue;
+        }
         double* mine = mb + lines_b;
         unsigned long long* from =
             b > 0 ? reinterpret_cast<unsigned long long*>(mb + lines_b - (long long)d.A * d.L)
                   : nullptr;
         const bool feeds = b + 1 < d.B;
-        line_phase1(a, d, s, qb, 0, lane, ends, fb);
+        bool live = true;  // false after a wait gave up: keep the hand-shake only
         for (int ch = 0; ch < d.A; ++ch) {
-          const long long q0 = qb + ch * d.sa;
-          __syncwarp();
-          if (b == 0) {  // the second pair's minus side is a halo
+          const int k = ch & 1;
+          const LineBuf lb = k ? buf1 : buf0;
+          named_sync(kBarFull0 + k, kTdmaBlock);
+          if (live) {
+            const long long q0 = qb + ch * d.sa;
             for (int e = lane; e < d.L; e += 32) {
-              const double t = s.rhs[e] + s.c2m[e] * __ldcg(phi + q0 + e * d.se - d.s2);
-              s.rhs[e] = t + s.c2t[e];
-            }
-          } else {  // the previous owner's line `ch`, from its mailbox
-            unsigned long long* slot = from + (long long)ch * d.L;
-            unsigned pend = 0;
-            for (int k = 0; lane + 32 * k < d.L; ++k) pend |= 1u << k;
-            uint64_t t0 = 0;
-            uint32_t spins = 0;
-            for (;;) {
-              for (int k = 0; lane + 32 * k < d.L; ++k) {
-                if (!(pend & (1u << k))) continue;
-                const int e = lane + 32 * k;
-                const unsigned long long v = ld_relaxed_u64(slot + e);
-                if (v == kEmptyBits) continue;
-                const double t = s.rhs[e] + s.c2m[e] * __longlong_as_double((long long)v);
-                s.rhs[e] = t + s.c2t[e];
-                slot[e] = kEmptyBits;
-                pend &= ~(1u << k);
+              const double p1m = ch == 0 ? lb.p1h[e] : s_x[e];
+              double t = lb.su[e] + lb.c1m[e] * p1m;
+              t = t + lb.c1t[e];
+              if (b == 0) {
+                t = t + lb.c2m[e] * lb.p2h[e];
+                t = t + lb.c2t[e];
               }
-              if (!__any_sync(0xffffffffu, pend != 0)) break;
-              if ((++spins & 63u) == 0) {
-                int stop = 0;
-                if (lane == 0) {
-                  if (spins == 64u) t0 = global_ns();
-                  if (ld_volatile_i32(a.ws.err) != 0) {
-                    stop = 1;
-                  } else if (global_ns() - t0 > a.timeout_ns) {
-                    atomicCAS(a.ws.err, 0, (int)EAF_ETIMEOUT);
-                    stop = 1;
-                  }
-                }
-                if (__shfl_sync(0xffffffffu, stop, 0)) break;
-              }
+              s_rhs[e] = t;
             }
-            if (__any_sync(0xffffffffu, pend != 0)) { ok = false; break; }
+            if (b > 0 && !take_mailbox(a, from + (long long)ch * d.L, lb, s_rhs, d.L, lane))
+              live = false;
+            __syncwarp();
+            if (live) {
+              if (lane == 0) {
+                // lagged couplings of the segment ends (:299-302, :325-328, :352-355)
+                s_rhs[0] = s_rhs[0] + s_ends[k][0];
+                s_rhs[d.L - 1] = s_rhs[d.L - 1] + s_ends[k][1];
+                thomas_line(lb, s_rhs, s_dp, s_x, d.L);
+              }
+              __syncwarp();
+              for (int e = lane; e < d.L; e += 32) {
+                const double xv = s_x[e];
+                if (feeds) mine[(long long)ch * d.L + e] = xv;
+                phi[q0 + e * d.se] = xv;
+              }
+              __syncwarp();
+            }
           }
-          __syncwarp();
-          if (lane == 0) {
-            // lagged couplings of the segment ends (:299-302, :325-328, :352-355)
-            s.rhs[0] = s.rhs[0] + ends[0];
-            s.rhs[d.L - 1] = s.rhs[d.L - 1] + ends[1];
-            thomas_line(s, d.L);
-          }
-          __syncwarp();
-          for (int e = lane; e < d.L; e += 32) {
-            const double xv = s.x[e];
-            if (feeds) mine[(long long)ch * d.L + e] = xv;
-            phi[q0 + e * d.se] = xv;
-          }
-          __syncwarp();
-          if (ch + 1 < d.A)
-            line_phase1(a, d, s, q0 + d.sa, ch + 1, lane, ends, fb + (long long)(ch + 1) * d.L);
+          if (ch + 2 < d.A) named_arrive(kBarEmpty0 + k, kTdmaBlock);
         }
       }
+      // A solver whose wait gave up kept the hand-shake and set the error
+      // word; the other waits see it and give up too, so every warp reaches
+      // the next group barrier and the launch ends with EAF_ETIMEOUT.
     }
   }
 }
@@ -543,7 +594,7 @@ cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, 
   a.ws = ws;
   a.timeout_ns = timeout_ns;
   const int grid = tdma_grid(nr, nth, nz);
-  const size_t smem = (size_t)9 * lmax * sizeof(double);
+  const size_t smem = (size_t)(2 * kBufArrays + 3) * lmax * sizeof(double);
   cudaError_t e = cudaSuccess;
   if (smem > 48 * 1024)
     e = cudaFuncSetAttribute((const void*)tdma_kernel,
@@ -560,7 +611,7 @@ cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, 
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
-  return cudaLaunchCooperativeKernel((const void*)tdma_kernel, dim3(grid), dim3(32), args,
+  return cudaLaunchCooperativeKernel((const void*)tdma_kernel, dim3(grid), dim3(kTdmaBlock), args,
                                      smem, st);
 }
 
