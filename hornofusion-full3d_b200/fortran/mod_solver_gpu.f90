@@ -14,13 +14,22 @@
 ! (src/mod_workspace.f90:120-126), so they pass to the C entry point without
 ! copies. Not compiled in this repository's build (no Fortran compiler is
 ! available where it is built); link with -L<dir> -leafcg.
+!
+! The same module replaces the line-by-line TDMA and the transport residual
+! of mod_solver_3d (tdma_3d_mpi, :252-366; compute_residual_3d_mpi,
+! :625-694) for their callers in momentum, energy, species, turbulence,
+! radiation and continuity (e.g. src/mod_momentum_3d.f90:326-329):
+!     residual = compute_residual_3d_gpu(aW, ..., Su, vel, m)
+!     call tdma_3d_gpu(aW, ..., Su, vel, m, cfg%max_inner_mom)
 !===============================================================================
 module mod_solver_gpu
     use iso_c_binding
     implicit none
     private
     public :: cg_3d_gpu, cg_3d_gpu_mixed, cg_gpu_release
+    public :: tdma_3d_gpu, compute_residual_3d_gpu
     public :: eaf_cg_create, eaf_cg_destroy, eaf_cg_solve_f64, eaf_cg_solve_mixed
+    public :: eaf_tdma_3d_f64, eaf_residual_3d_f64
 
     integer(c_int), parameter, public :: EAF_OK = 0, EAF_ENONFINITE = 3
 
@@ -64,6 +73,26 @@ module mod_solver_gpu
             real(c_double), intent(out) :: residual
             integer(c_int), intent(out) :: n_iter, n_outer
         end function eaf_cg_solve_mixed
+
+        integer(c_int) function eaf_tdma_3d_f64(h, aW, aE, aS, aN, aB, aT, aP, &
+                Su, phi, n_sweep) bind(C, name="eaf_tdma_3d_f64")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: aW(*), aE(*), aS(*), aN(*)
+            real(c_double), intent(in) :: aB(*), aT(*), aP(*), Su(*)
+            real(c_double), intent(inout) :: phi(*)
+            integer(c_int), value :: n_sweep
+        end function eaf_tdma_3d_f64
+
+        integer(c_int) function eaf_residual_3d_f64(h, aW, aE, aS, aN, aB, aT, aP, &
+                Su, phi, residual) bind(C, name="eaf_residual_3d_f64")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: aW(*), aE(*), aS(*), aN(*)
+            real(c_double), intent(in) :: aB(*), aT(*), aP(*), Su(*)
+            real(c_double), intent(in) :: phi(*)
+            real(c_double), intent(out) :: residual
+        end function eaf_residual_3d_f64
     end interface
 
     ! One handle per mesh size, kept across SIMPLE iterations like the
@@ -137,6 +166,46 @@ contains
         residual = res
         n_iter = nit
     end subroutine cg_3d_gpu_mixed
+
+    ! Same dummies as tdma_3d_mpi; serial meshes only. phi comes back
+    ! bit-identical to the serial routine's.
+    subroutine tdma_3d_gpu(aW, aE, aS, aN, aB, aT, aP, Su, phi, m, n_sweep)
+        use mod_constants, only: dp
+        use mod_types_3d, only: mesh_t
+        real(dp), intent(in), contiguous  :: aW(-1:,-1:,-1:), aE(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aS(-1:,-1:,-1:), aN(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aB(-1:,-1:,-1:), aT(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aP(-1:,-1:,-1:), Su(-1:,-1:,-1:)
+        real(dp), intent(inout), contiguous :: phi(-1:,-1:,-1:)
+        type(mesh_t), intent(in) :: m
+        integer, intent(in)      :: n_sweep
+        integer(c_int) :: st
+        if (m%is_parallel) error stop 'tdma_3d_gpu: decomposed meshes are not supported'
+        call ensure_handle(m%nr, m%ntheta, m%nz)
+        st = eaf_tdma_3d_f64(handle, aW, aE, aS, aN, aB, aT, aP, Su, phi, &
+                             int(n_sweep, c_int))
+        if (st /= EAF_OK) error stop 'eaf_tdma_3d_f64 failed'
+    end subroutine tdma_3d_gpu
+
+    ! Same dummies and result as compute_residual_3d_mpi; serial meshes only.
+    function compute_residual_3d_gpu(aW, aE, aS, aN, aB, aT, aP, Su, phi, m) result(res)
+        use mod_constants, only: dp
+        use mod_types_3d, only: mesh_t
+        real(dp), intent(in), contiguous :: aW(-1:,-1:,-1:), aE(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous :: aS(-1:,-1:,-1:), aN(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous :: aB(-1:,-1:,-1:), aT(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous :: aP(-1:,-1:,-1:), Su(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous :: phi(-1:,-1:,-1:)
+        type(mesh_t), intent(in) :: m
+        real(dp) :: res
+        integer(c_int) :: st
+        real(c_double) :: r
+        if (m%is_parallel) error stop 'compute_residual_3d_gpu: decomposed meshes are not supported'
+        call ensure_handle(m%nr, m%ntheta, m%nz)
+        st = eaf_residual_3d_f64(handle, aW, aE, aS, aN, aB, aT, aP, Su, phi, r)
+        if (st /= EAF_OK) error stop 'eaf_residual_3d_f64 failed'
+        res = r
+    end function compute_residual_3d_gpu
 
     subroutine cg_gpu_release()
         integer(c_int) :: st
