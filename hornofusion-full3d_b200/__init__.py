@@ -129,6 +129,40 @@ class CGSolver:
         check(st, "eaf_residual_3d_f64")
         return res.value
 
+    def pressure_correct(self, fields, device_ptrs: bool = False) -> None:
+        """Post-CG corrections of the pressure step (src/mod_pressure_3d.f90:
+        333-397, correct_velocities :689-746) in place on the arrays of
+        ``fields`` (an object with the attributes of eafgen.PcorrFields:
+        float64 halo-layout arrays, int32 flag/mask arrays, coordinate
+        arrays, ``has_gas``, ``alpha_p``)."""
+        from ._lib import PcorrFieldsC, PhaseFields
+
+        def addr(a, kind):
+            if isinstance(a, np.ndarray):
+                want = np.float64 if kind == "d" else np.int32
+                if a.dtype != want or not a.flags.c_contiguous:
+                    raise ValueError(f"array must be C-contiguous {np.dtype(want)}")
+                return a.ctypes.data
+            if hasattr(a, "data_ptr"):
+                return a.data_ptr()
+            raise TypeError(f"unsupported array type {type(a)!r}")
+
+        c = PcorrFieldsC()
+        for n in ("pp", "Fs_r", "Fs_th", "Fs_z", "ac_r", "ac_th", "ac_z", "Fc_r", "Fc_th",
+                  "Fc_z", "vol", "r", "theta", "z", "p"):
+            setattr(c, n, addr(getattr(fields, n), "d"))
+        for n in ("lk_r", "lk_th", "lk_z", "cell_type", "act_l", "act_g"):
+            setattr(c, n, addr(getattr(fields, n), "i"))
+        for ph in ("liq", "gas") if fields.has_gas else ("liq",):
+            pf = PhaseFields(*[addr(getattr(fields, ph + "_" + n), "d") for n in
+                               ("alpha", "aP_ur", "aP_uth", "aP_uz", "ur", "uth", "uz")])
+            setattr(c, ph, pf)
+        c.has_gas = 1 if fields.has_gas else 0
+        c.alpha_p = float(fields.alpha_p)
+        fn = (self._lib.eaf_pressure_correct_f64_device if device_ptrs
+              else self._lib.eaf_pressure_correct_f64)
+        check(fn(self._h, ctypes.byref(c)), "eaf_pressure_correct_f64")
+
     def solve_mixed(self, arrays, phi, tol: float = SOR_TOL_PRESSURE,
                     inner_tol: float = 0.1, max_outer: int = 200,
                     max_inner: int = 100000, device_ptrs: bool = False):

@@ -33,6 +33,23 @@ class SrvStats(ctypes.Structure):
                 ("p50_ms", "p99_ms", "mean_ms", "max_ms", "solves_per_s",
                  "mean_batch", "used_bytes", "budget_bytes")]
 
+class PhaseFields(ctypes.Structure):
+    """eaf_phase_fields_t"""
+    _fields_ = [(n, ctypes.c_void_p) for n in
+                ("alpha", "aP_ur", "aP_uth", "aP_uz", "ur", "uth", "uz")]
+
+
+class PcorrFieldsC(ctypes.Structure):
+    """eaf_pcorr_fields_t"""
+    _fields_ = ([(n, ctypes.c_void_p) for n in
+                 ("pp", "Fs_r", "Fs_th", "Fs_z", "ac_r", "ac_th", "ac_z", "Fc_r",
+                  "Fc_th", "Fc_z", "vol", "r", "theta", "z", "p")]
+                + [("liq", PhaseFields), ("gas", PhaseFields)]
+                + [(n, ctypes.c_void_p) for n in
+                   ("lk_r", "lk_th", "lk_z", "cell_type", "act_l", "act_g")]
+                + [("has_gas", ctypes.c_int), ("alpha_p", ctypes.c_double)])
+
+
 STATUS_NAMES = {
     0: "EAF_OK", 1: "EAF_ECUDA", 2: "EAF_EINVAL", 3: "EAF_ENONFINITE",
     4: "EAF_ETIMEOUT", 5: "EAF_EUNSUPPORTED", 6: "EAF_ENOMEM", 7: "EAF_EADMIT",
@@ -57,6 +74,8 @@ SIGNATURES = [
     ("eaf_tdma_3d_f64", _ci, [_vp] + _A8 + [_vp, _ci]),
     ("eaf_tdma_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _ci]),
     ("eaf_residual_3d_f64", _ci, [_vp] + _A8 + [_vp, _pd]),
+    ("eaf_pressure_correct_f64", _ci, [_vp, _vp]),
+    ("eaf_pressure_correct_f64_device", _ci, [_vp, _vp]),
     ("eaf_residual_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _pd]),
     ("eaf_cg_solve_mixed", _ci,
      [_vp] + _A8 + [_vp, _ci, _ci, _cd, _cd, _pd, _pi, _pi]),

@@ -37,6 +37,7 @@ UNITS = {
     "serve.cu": [],
     "diag.cu": [],
     "tdma.cu": ["-fmad=false"],
+    "pcorr.cu": ["-fmad=false"],
 }
 
 

@@ -48,6 +48,8 @@ struct eaf_cg {
   int last_grid, last_block;
   double* tdma_mbox;  // TDMA line hand-over slots (lazy)
   double* tdma_fac;  // TDMA line factors (lazy)
+  double* pc_d;      // post-CG correction mirror: doubles (lazy)
+  int* pc_i;         // post-CG correction mirror: ints (lazy)
 };
 
 namespace eaf {
@@ -99,6 +101,8 @@ static void free_handle(eaf_cg* h) {
   cudaFree(h->ws.result);
   cudaFree(h->tdma_mbox);
   cudaFree(h->tdma_fac);
+  cudaFree(h->pc_d);
+  cudaFree(h->pc_i);
   if (h->res_h) cudaFreeHost(h->res_h);
   for (int i = 0; i < 6; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -488,6 +492,39 @@ int run_residual(eaf_cg* h, const HaloInputs& in, const double* phi, double* res
   return h->res_h->status;
 }
 
+// ---------------------------------------------------------------------------
+// Post-CG corrections.
+// ---------------------------------------------------------------------------
+constexpr int kPcHalo = 26;  // halo double arrays of the mirror
+constexpr int kPcInts = 6;
+
+bool pcorr_fields_ok(const eaf_pcorr_fields_t* f) {
+  if (!f) return false;
+  const void* req[] = {f->pp,     f->Fs_r,   f->Fs_th,  f->Fs_z,      f->ac_r,
+                       f->ac_th,  f->ac_z,   f->Fc_r,   f->Fc_th,     f->Fc_z,
+                       f->vol,    f->r,      f->theta,  f->z,         f->p,
+                       f->liq.alpha, f->liq.aP_ur, f->liq.aP_uth, f->liq.aP_uz,
+                       f->liq.ur, f->liq.uth, f->liq.uz, f->lk_r,    f->lk_th,
+                       f->lk_z,   f->cell_type, f->act_l, f->act_g};
+  for (const void* q : req)
+    if (!q) return false;
+  if (f->has_gas) {
+    const void* gas[] = {f->gas.alpha, f->gas.aP_ur, f->gas.aP_uth, f->gas.aP_uz,
+                         f->gas.ur,    f->gas.uth,   f->gas.uz};
+    for (const void* q : gas)
+      if (!q) return false;
+  }
+  return true;
+}
+
+int run_pcorr(eaf_cg* h, const eaf_pcorr_fields_t& f) {
+  EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
+  EAF_CUDA(eaf::launch_pcorr_f64(f, h->nr, h->nth, h->nz, h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[3], h->st));
+  h->last_kernels = 3;
+  return EAF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -626,6 +663,93 @@ int eaf_residual_3d_f64_device(eaf_cg_t h, const double* aW, const double* aE,
   eaf::DeviceGuard guard(h->device);
   HaloInputs in = {arr[0], arr[1], arr[2], arr[3], arr[4], arr[5], arr[6], arr[7], phi};
   return run_residual(h, in, phi, residual);
+}
+
+int eaf_pressure_correct_f64_device(eaf_cg_t h, const eaf_pcorr_fields_t* f) {
+  if (!h || !pcorr_fields_ok(f)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  eaf_pcorr_fields_t d = *f;
+  if (!d.has_gas) d.gas = eaf_phase_fields_t{};
+  int rc = run_pcorr(h, d);
+  if (rc != EAF_OK) return rc;
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
+  return EAF_OK;
+}
+
+int eaf_pressure_correct_f64(eaf_cg_t h, const eaf_pcorr_fields_t* f) {
+  if (!h || !pcorr_fields_ok(f)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  const size_t nh = h->nh;
+  const size_t nc = (size_t)(h->nr + 4) + (h->nth + 4) + (h->nz + 4);
+  if (!h->pc_d) {
+    EAF_CUDA(cudaMalloc((void**)&h->pc_d, sizeof(double) * (kPcHalo * nh + nc)));
+  }
+  if (!h->pc_i) {
+    EAF_CUDA(cudaMalloc((void**)&h->pc_i, sizeof(int) * kPcInts * nh));
+  }
+  double* D = h->pc_d;
+  int* I = h->pc_i;
+  eaf_pcorr_fields_t d = *f;
+  // mirror slots: 0 pp, 1-3 Fs, 4-6 ac, 7-9 Fc, 10 vol, 11 p, 12-18 liq, 19-25 gas
+  const double* src_in[] = {f->pp, f->Fs_r, f->Fs_th, f->Fs_z, f->ac_r, f->ac_th,
+                            f->ac_z, f->Fc_r, f->Fc_th, f->Fc_z, f->vol, f->p,
+                            f->liq.alpha, f->liq.aP_ur, f->liq.aP_uth, f->liq.aP_uz,
+                            f->liq.ur, f->liq.uth, f->liq.uz,
+                            f->gas.alpha, f->gas.aP_ur, f->gas.aP_uth, f->gas.aP_uz,
+                            f->gas.ur, f->gas.uth, f->gas.uz};
+  const int n_in = f->has_gas ? 26 : 19;
+  EAF_CUDA(cudaEventRecord(h->ev[0], h->st));
+  for (int i = 0; i < n_in; ++i)
+    EAF_CUDA(cudaMemcpyAsync(D + (size_t)i * nh, src_in[i], nh * sizeof(double),
+                             cudaMemcpyHostToDevice, h->st));
+  double* coords = D + (size_t)kPcHalo * nh;
+  EAF_CUDA(cudaMemcpyAsync(coords, f->r, (h->nr + 4) * sizeof(double),
+                           cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4, f->theta, (h->nth + 4) * sizeof(double),
+                           cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4 + h->nth + 4, f->z,
+                           (h->nz + 4) * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  const int* src_i[] = {f->lk_r, f->lk_th, f->lk_z, f->cell_type, f->act_l, f->act_g};
+  for (int i = 0; i < kPcInts; ++i)
+    EAF_CUDA(cudaMemcpyAsync(I + (size_t)i * nh, src_i[i], nh * sizeof(int),
+                             cudaMemcpyHostToDevice, h->st));
+  auto slot = [&](int i) { return D + (size_t)i * nh; };
+  d.pp = slot(0);
+  d.Fs_r = slot(1); d.Fs_th = slot(2); d.Fs_z = slot(3);
+  d.ac_r = slot(4); d.ac_th = slot(5); d.ac_z = slot(6);
+  d.Fc_r = slot(7); d.Fc_th = slot(8); d.Fc_z = slot(9);
+  d.vol = slot(10); d.p = slot(11);
+  d.liq = eaf_phase_fields_t{slot(12), slot(13), slot(14), slot(15), slot(16), slot(17),
+                             slot(18)};
+  d.gas = f->has_gas ? eaf_phase_fields_t{slot(19), slot(20), slot(21), slot(22), slot(23),
+                                          slot(24), slot(25)}
+                     : eaf_phase_fields_t{};
+  d.r = coords;
+  d.theta = coords + h->nr + 4;
+  d.z = coords + h->nr + 4 + h->nth + 4;
+  d.lk_r = I; d.lk_th = I + nh; d.lk_z = I + 2 * nh;
+  d.cell_type = I + 3 * nh; d.act_l = I + 4 * nh; d.act_g = I + 5 * nh;
+  int rc = run_pcorr(h, d);
+  if (rc != EAF_OK) return rc;
+  double* dst_out[] = {f->Fc_r, f->Fc_th, f->Fc_z, f->p, f->liq.ur, f->liq.uth, f->liq.uz,
+                       f->gas.ur, f->gas.uth, f->gas.uz};
+  const int slots_out[] = {7, 8, 9, 11, 16, 17, 18, 23, 24, 25};
+  const int n_out = f->has_gas ? 10 : 7;
+  for (int i = 0; i < n_out; ++i)
+    EAF_CUDA(cudaMemcpyAsync(dst_out[i], slot(slots_out[i]), nh * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->st));
+  int* lk_out[] = {f->lk_r, f->lk_th, f->lk_z};
+  for (int i = 0; i < 3; ++i)
+    EAF_CUDA(cudaMemcpyAsync(lk_out[i], I + (size_t)i * nh, nh * sizeof(int),
+                             cudaMemcpyDeviceToHost, h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[5], h->st));
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
+  if (cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]) == cudaSuccess) h->last_e2e_ms = ms;
+  return EAF_OK;
 }
 
 }  // extern "C"

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include "cg_common.cuh"
+#include "eafcg.h"
 
 namespace eaf {
 
@@ -146,6 +147,11 @@ const void* residual_kernel_ptr();
 // from `/` in any bit, counts[1] = pairs that took its fast path.
 cudaError_t run_div_check(long long n, unsigned long long seed, unsigned long long* counts,
                           cudaStream_t st);
+
+// Post-CG corrections (solve_pressure_correction after the CG), three
+// launches on `st`; every pointer of `f` is a device pointer.
+cudaError_t launch_pcorr_f64(const eaf_pcorr_fields_t& f, int nr, int nth, int nz,
+                             cudaStream_t st);
 
 // Threads per block of the batched kernels (FP64 and mixed).
 constexpr int kBatchBlock = 512;

@@ -328,6 +328,92 @@ def make_transport_system(nr: int, nth: int, nz: int, seed: int = 0,
     return System(nr=nr, nth=nth, nz=nz, **out)
 
 
+# Post-CG correction fields (solve_pressure_correction after the CG):
+# double arrays in the halo layout, the coordinate arrays (index -1..n+2),
+# int arrays (flags and Fortran default logicals), and per-phase fields.
+PCORR_DOUBLES = ("pp", "Fs_r", "Fs_th", "Fs_z", "ac_r", "ac_th", "ac_z",
+                 "Fc_r", "Fc_th", "Fc_z", "vol", "r", "theta", "z", "p")
+PCORR_PHASE = ("alpha", "aP_ur", "aP_uth", "aP_uz", "ur", "uth", "uz")
+PCORR_INTS = ("lk_r", "lk_th", "lk_z", "cell_type", "act_l", "act_g")
+P_HYDRO_CAP = 2.0e6
+
+
+class PcorrFields:
+    """Every array the post-CG corrections read or write, for one mesh."""
+
+    def __init__(self, nr, nth, nz, has_gas, alpha_p):
+        self.nr, self.nth, self.nz = nr, nth, nz
+        self.has_gas = has_gas
+        self.alpha_p = alpha_p
+
+    def copy(self):
+        c = PcorrFields(self.nr, self.nth, self.nz, self.has_gas, self.alpha_p)
+        for k, v in self.__dict__.items():
+            if isinstance(v, np.ndarray):
+                setattr(c, k, v.copy())
+        return c
+
+    def doubles(self):
+        """The oracle's ordered double arrays (22 + 7 gas)."""
+        out = [getattr(self, n) for n in PCORR_DOUBLES]
+        out += [getattr(self, "liq_" + n) for n in PCORR_PHASE]
+        out += [getattr(self, "gas_" + n) for n in PCORR_PHASE]
+        return out
+
+    def ints(self):
+        return [getattr(self, n) for n in PCORR_INTS]
+
+    def outputs(self):
+        names = ["Fc_r", "Fc_th", "Fc_z", "p", "lk_r", "lk_th", "lk_z"]
+        names += ["liq_ur", "liq_uth", "liq_uz"]
+        if self.has_gas:
+            names += ["gas_ur", "gas_uth", "gas_uz"]
+        return {n: getattr(self, n) for n in names}
+
+
+def make_pcorr_fields(nr: int, nth: int, nz: int, seed: int = 0, has_gas: bool = True,
+                      solid_frac: float = 0.05, sealed_frac: float = 0.08,
+                      alpha_p: float = 0.7) -> PcorrFields:
+    """Seeded inputs of the post-CG corrections: pp and the assembly's
+    face terms Fs/ac (random), link flags mostly 1, a few solid cells
+    (cell_type 0), liquid/gas activity masks leaving `sealed_frac` of the
+    cells in neither phase, positive volumes, uniform cell centres (r, theta,
+    z with halo entries), phase fields with some momentum diagonals at or
+    below SMALL (their correction is skipped) and p with some values beyond
+    +-P_HYDRO_CAP (clamped). Halo entries are random too."""
+    rng = np.random.default_rng(seed)
+    shp = halo_shape(nr, nth, nz)
+    f = PcorrFields(nr, nth, nz, has_gas, alpha_p)
+    f.pp = rng.normal(0.0, 1e3, size=shp)
+    for n in ("Fs_r", "Fs_th", "Fs_z", "Fc_r", "Fc_th", "Fc_z"):
+        setattr(f, n, rng.normal(0.0, 1.0, size=shp))
+    for n in ("ac_r", "ac_th", "ac_z"):
+        setattr(f, n, rng.uniform(0.0, 1e-3, size=shp))
+    f.vol = rng.uniform(0.5, 1.5, size=shp) * 1e-2
+    f.r = (np.arange(-1, nr + 3) - 0.5) * (R_FURNACE / nr)
+    f.theta = (np.arange(-1, nth + 3) - 0.5) * (2.0 * math.pi / nth)
+    f.z = (np.arange(-1, nz + 3) - 0.5) * (H_FURNACE / nz)
+    f.p = rng.normal(0.0, 1e6, size=shp)
+    f.p[rng.random(shp) < 0.05] *= 5.0
+    for ph in ("liq", "gas"):
+        setattr(f, ph + "_alpha", rng.uniform(0.0, 1.0, size=shp))
+        for c in ("aP_ur", "aP_uth", "aP_uz"):
+            a = rng.uniform(1.0, 1e3, size=shp)
+            a[rng.random(shp) < 0.05] = 1e-31
+            setattr(f, ph + "_" + c, a)
+        for c in ("ur", "uth", "uz"):
+            setattr(f, ph + "_" + c, rng.normal(0.0, 1.0, size=shp))
+    for n in ("lk_r", "lk_th", "lk_z"):
+        setattr(f, n, (rng.random(shp) < 0.9).astype(np.int32))
+    f.cell_type = (rng.random(shp) >= solid_frac).astype(np.int32)
+    u = rng.random(shp)
+    f.act_l = (u < 0.6).astype(np.int32)
+    f.act_g = ((u >= 0.6) & (u < 1.0 - sealed_frac)).astype(np.int32)
+    f.act_g[rng.random(shp) < 0.2] = 1
+    f.act_g[u >= 1.0 - sealed_frac] = 0
+    return f
+
+
 def system_bytes(nr: int, nth: int, nz: int) -> int:
     """Host bytes of one system (8 halo-layout FP64 arrays)."""
     return 8 * 8 * (nr + 4) * (nth + 4) * (nz + 4)

@@ -163,6 +163,55 @@ int eaf_residual_3d_f64_device(eaf_cg_t h, const double* aW, const double* aE,
                                const double* aT, const double* aP, const double* Su,
                                const double* phi, double* residual);
 
+/* Post-CG corrections of the pressure-correction step: replaces the serial
+ * code after the CG in solve_pressure_correction
+ * (src/mod_pressure_3d.f90:333-397) with correct_velocities (:689-746):
+ *   1. conservative face fluxes Fc = Fs + ac (pp_P - pp_nb) where linked
+ *      (lk == 1) in non-solid cells; theta halos of Fc and lk refreshed;
+ *   2. velocity corrections u -= (alpha V / aP_u) dpp/dx of the liquid in
+ *      its active cells, then of the gas (has_gas) in its active cells;
+ *   3. p = clamp(p + alpha_p pp, +-2e6) over the whole array;
+ *   4. sealed cells (non-solid, neither phase active): p = mean of their
+ *      active neighbours' p, 0 if none; theta halos of p refreshed.
+ * Results are bit-identical to the serial Fortran (the clamp of a NaN p is
+ * not pinned). Every 3-D array is in the CG's halo layout; r, theta and z
+ * are the cell-centre coordinates with halo entries (n + 4 values from
+ * index -1); int arrays are Fortran default integers/logicals (nonzero =
+ * true). The gas fields may be NULL when has_gas is 0. */
+typedef struct {
+  const double* alpha;   /* volume fraction */
+  const double* aP_ur;   /* momentum diagonals */
+  const double* aP_uth;
+  const double* aP_uz;
+  double* ur;            /* velocities, corrected in place */
+  double* uth;
+  double* uz;
+} eaf_phase_fields_t;
+
+typedef struct {
+  const double* pp;                       /* the CG solution */
+  const double *Fs_r, *Fs_th, *Fs_z;      /* predicted face fluxes */
+  const double *ac_r, *ac_th, *ac_z;      /* face links */
+  double *Fc_r, *Fc_th, *Fc_z;            /* conservative fluxes, in/out */
+  const double* vol;                      /* cell volumes */
+  const double *r, *theta, *z;            /* cell centres, index -1..n+2 */
+  double* p;                              /* pressure, in/out */
+  eaf_phase_fields_t liq;
+  eaf_phase_fields_t gas;
+  int *lk_r, *lk_th, *lk_z;               /* face link flags (halos refreshed) */
+  const int* cell_type;                   /* 0 = solid */
+  const int *act_l, *act_g;               /* phase activity masks */
+  int has_gas;                            /* gas phase in the pressure equation */
+  double alpha_p;                         /* pressure under-relaxation */
+} eaf_pcorr_fields_t;
+
+/* Host arrays: uploads the fields to the handle's device mirror (allocated
+ * on first use), corrects, downloads the in/out arrays. */
+int eaf_pressure_correct_f64(eaf_cg_t h, const eaf_pcorr_fields_t* f);
+/* Device arrays, corrected in place on the handle's stream (synchronised
+ * before return). */
+int eaf_pressure_correct_f64_device(eaf_cg_t h, const eaf_pcorr_fields_t* f);
+
 /* Bound on every device-side barrier wait, in milliseconds (default 2000). */
 int eaf_cg_set_timeout_ms(eaf_cg_t h, double ms);
 

@@ -51,6 +51,10 @@ def lib():
         L.eaf_oracle_tdma_3d.restype = ci
         L.eaf_oracle_residual_3d.argtypes = [ci, ci, ci] + [_dp] * 9 + [ci, ci]
         L.eaf_oracle_residual_3d.restype = cd
+        L.eaf_oracle_pressure_correct.argtypes = [ci, ci, ci, ctypes.POINTER(_dp),
+                                                  ctypes.POINTER(ctypes.POINTER(ci)),
+                                                  ci, cd]
+        L.eaf_oracle_pressure_correct.restype = ci
         L.eaf_oracle_max_threads.argtypes = []
         L.eaf_oracle_max_threads.restype = ci
         _lib = L
@@ -118,6 +122,24 @@ def residual_3d(system, phi: np.ndarray, plan: tuple | None = None) -> float:
     G, B = plan if plan is not None else (0, 0)
     args = [system.nr, system.nth, system.nz] + [_p(a) for a in system.arrays()]
     return lib().eaf_oracle_residual_3d(*args, _p(phi), int(G), int(B))
+
+
+def pressure_correct(f) -> None:
+    """Serial post-CG corrections (src/mod_pressure_3d.f90:333-397, 689-746)
+    in place on the arrays of an eafgen.PcorrFields."""
+    ci = ctypes.c_int
+    dv = f.doubles()
+    iv = f.ints()
+    for a in dv:
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    for a in iv:
+        assert a.dtype == np.int32 and a.flags.c_contiguous
+    darr = (_dp * len(dv))(*[a.ctypes.data_as(_dp) for a in dv])
+    iarr = (ctypes.POINTER(ci) * len(iv))(*[a.ctypes.data_as(ctypes.POINTER(ci)) for a in iv])
+    rc = lib().eaf_oracle_pressure_correct(f.nr, f.nth, f.nz, darr, iarr,
+                                           1 if f.has_gas else 0, float(f.alpha_p))
+    if rc != 0:
+        raise RuntimeError(f"oracle pressure_correct failed with status {rc}")
 
 
 def max_threads() -> int:

@@ -36,7 +36,12 @@
  *   - tdma_3d_mpi, line-by-line TDMA sweeps ......... src/mod_solver_3d.f90:252-366
  *     with the 1D Thomas solve `tdma` .............. src/mod_solver_3d.f90:22-46
  *   - compute_residual_3d_mpi ....................... src/mod_solver_3d.f90:625-694
- * (see eaf_oracle_tdma_3d and eaf_oracle_residual_3d below).
+ * (see eaf_oracle_tdma_3d and eaf_oracle_residual_3d below), and the serial
+ * post-CG corrections of solve_pressure_correction
+ *   - flux export, halo refresh, velocity and pressure corrections, sealed
+ *     cells ..................................... src/mod_pressure_3d.f90:333-397
+ *   - correct_velocities ........................ src/mod_pressure_3d.f90:689-746
+ * (eaf_oracle_pressure_correct).
  *
  * PARITY UNPINNED: the reference is Fortran + MPI and no Fortran compiler or
  * MPI exists where this is built or run, and the reference's tests pin only
@@ -598,4 +603,127 @@ double eaf_oracle_residual_3d(int nr, int nth, int nz, const double* aW, const d
         free(part);
     }
     return sqrt(sum_r) / (sqrt(sum_b) + SMALL);
+}
+
+/* ------------------------------------------------------------------------
+ * Post-CG corrections of solve_pressure_correction, serial branch
+ * (src/mod_pressure_3d.f90:333-397, correct_velocities :689-746), in the
+ * reference's statement order:
+ *   1. conservative face fluxes Fc = Fs + ac (pp_P - pp_nb) where linked;
+ *   2. theta-halo refresh of Fc_r/th/z and of the link flags (int);
+ *   3. correct_velocities of the liquid (act_l), then of the gas (act_g)
+ *      when it is in the pressure equation;
+ *   4. p = p + alpha_p pp and p = max(-P_HYDRO_CAP, min(P_HYDRO_CAP, p)),
+ *      both over the whole array (halos included);
+ *   5. sealed cells (neither phase active): p = mean of the p of their
+ *      active neighbours (i-1, i+1, j-1, j+1, k-1, k+1 in that order), 0
+ *      without any;
+ *   6. theta-halo refresh of p.
+ * Fortran min/max are written fmin/fmax (identical on non-NaN values; the
+ * result for a NaN p is not pinned). Logical masks are default-kind
+ * Fortran logicals (4 bytes, nonzero = true).
+ * dv: pp, Fs_r, Fs_th, Fs_z, ac_r, ac_th, ac_z, Fc_r, Fc_th, Fc_z, vol,
+ *     r, theta, z (cell centres, index -1..n+2), p, then per phase (liquid,
+ *     gas) alpha, aP_ur, aP_uth, aP_uz, ur, uth, uz.
+ * iv: lk_r, lk_th, lk_z, cell_type, act_l, act_g.
+ * ---------------------------------------------------------------------- */
+#define P_HYDRO_CAP 2.0e6
+
+static void theta_wrap_int(const dims_t* d, int* x) {
+    for (int k = -1; k <= d->nz + 2; ++k)
+        for (int i = -1; i <= d->nr + 2; ++i) x[at(d, i, 0, k)] = x[at(d, i, d->nth, k)];
+    for (int k = -1; k <= d->nz + 2; ++k)
+        for (int i = -1; i <= d->nr + 2; ++i) x[at(d, i, -1, k)] = x[at(d, i, d->nth - 1, k)];
+    for (int k = -1; k <= d->nz + 2; ++k)
+        for (int i = -1; i <= d->nr + 2; ++i) x[at(d, i, d->nth + 1, k)] = x[at(d, i, 1, k)];
+    for (int k = -1; k <= d->nz + 2; ++k)
+        for (int i = -1; i <= d->nr + 2; ++i) x[at(d, i, d->nth + 2, k)] = x[at(d, i, 2, k)];
+}
+
+static void correct_velocities(const dims_t* d, double* const* ph, const double* pp,
+                               const double* vol, const double* r, const double* th,
+                               const double* z, const int* ct, const int* act) {
+    const double *alpha = ph[0], *aur = ph[1], *auth = ph[2], *auz = ph[3];
+    double *ur = ph[4], *uth = ph[5], *uz = ph[6];
+    for (int k = 1; k <= d->nz; ++k)
+        for (int j = 1; j <= d->nth; ++j)
+            for (int i = 1; i <= d->nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (ct[q] == 0) continue;
+                if (!act[q]) continue;
+                const int skip_r = (i == 1) || (i == d->nr);
+                if (!skip_r && fabs(aur[q]) > SMALL) {
+                    double dc = alpha[q] * vol[q] / aur[q];
+                    ur[q] = ur[q] - dc * (pp[q + 1] - pp[q - 1]) / (r[i + 2] - r[i]);
+                }
+                if (fabs(auth[q]) > SMALL) {
+                    double dc = alpha[q] * vol[q] / auth[q];
+                    uth[q] = uth[q] - dc * (pp[q + d->sx] - pp[q - d->sx]) /
+                                          (r[i + 1] * (th[j + 2] - th[j]));
+                }
+                const int skip_z = (k == 1) || (k == d->nz);
+                if (!skip_z && fabs(auz[q]) > SMALL) {
+                    double dc = alpha[q] * vol[q] / auz[q];
+                    uz[q] = uz[q] - dc * (pp[q + d->sxy] - pp[q - d->sxy]) / (z[k + 2] - z[k]);
+                }
+            }
+}
+
+int eaf_oracle_pressure_correct(int nr, int nth, int nz, double* const* dv, int* const* iv,
+                                int has_gas, double alpha_p) {
+    if (nr < 1 || nth < 1 || nz < 1) return 2;
+    const dims_t D = mkdims(nr, nth, nz);
+    const dims_t* d = &D;
+    const double *pp = dv[0], *Fs_r = dv[1], *Fs_th = dv[2], *Fs_z = dv[3], *ac_r = dv[4],
+                 *ac_th = dv[5], *ac_z = dv[6], *vol = dv[10], *r = dv[11], *th = dv[12],
+                 *z = dv[13];
+    double *Fc_r = dv[7], *Fc_th = dv[8], *Fc_z = dv[9], *p = dv[14];
+    int *lk_r = iv[0], *lk_th = iv[1], *lk_z = iv[2];
+    const int *ct = iv[3], *act_l = iv[4], *act_g = iv[5];
+    /* 1. (:333-345) */
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= nth; ++j)
+            for (int i = 1; i <= nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (ct[q] == 0) continue;
+                if (lk_r[q] == 1) Fc_r[q] = Fs_r[q] + ac_r[q] * (pp[q] - pp[q + 1]);
+                if (lk_th[q] == 1) Fc_th[q] = Fs_th[q] + ac_th[q] * (pp[q] - pp[q + d->sx]);
+                if (lk_z[q] == 1) Fc_z[q] = Fs_z[q] + ac_z[q] * (pp[q] - pp[q + d->sxy]);
+            }
+    /* 2. (:346-351) */
+    eaf_oracle_theta_wrap(nr, nth, nz, Fc_r);
+    eaf_oracle_theta_wrap(nr, nth, nz, Fc_th);
+    eaf_oracle_theta_wrap(nr, nth, nz, Fc_z);
+    theta_wrap_int(d, lk_r);
+    theta_wrap_int(d, lk_th);
+    theta_wrap_int(d, lk_z);
+    /* 3. (:354-356) */
+    correct_velocities(d, dv + 15, pp, vol, r, th, z, ct, act_l);
+    if (has_gas) correct_velocities(d, dv + 22, pp, vol, r, th, z, ct, act_g);
+    /* 4. (:358-360) */
+    for (size_t q = 0; q < d->n; ++q) p[q] = p[q] + alpha_p * pp[q];
+    for (size_t q = 0; q < d->n; ++q) p[q] = fmax(-P_HYDRO_CAP, fmin(P_HYDRO_CAP, p[q]));
+    /* 5. (:373-395, acc_nb :451-458) */
+    static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0},
+                                  {0, 0, -1}, {0, 0, 1}};
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= nth; ++j)
+            for (int i = 1; i <= nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (ct[q] == 0) continue;
+                if (act_l[q] || act_g[q]) continue;
+                double psum = 0.0;
+                int nnb = 0;
+                for (int t = 0; t < 6; ++t) {
+                    const size_t b = at(d, i + off[t][0], j + off[t][1], k + off[t][2]);
+                    if (ct[b] == 0) continue;
+                    if (!act_l[b] && !act_g[b]) continue;
+                    psum = psum + p[b];
+                    nnb = nnb + 1;
+                }
+                p[q] = nnb > 0 ? psum / (double)nnb : 0.0;
+            }
+    /* 6. (:396) */
+    eaf_oracle_theta_wrap(nr, nth, nz, p);
+    return 0;
 }
