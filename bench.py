@@ -490,6 +490,77 @@ def run_tdma(args):
     return 0
 
 
+PCORR_BYTES_PER_CELL = 300  # reads 23 doubles + 6 ints, writes 10 doubles (update + sealed pass)
+
+
+def run_pcorr(args):
+    """Post-CG corrections of the pressure step (solve_pressure_correction
+    after the CG) on the 60x120x84 mesh, liquid and gas phases, with the
+    fields resident on the device (value, HBM roofline) and through the
+    host-pointer entry (e2e); the single-thread CPU restatement as baseline."""
+    import numpy as np
+    import torch
+    eaf = importlib.import_module(PKG)
+    g = importlib.import_module(PKG + ".eafgen")
+    nr, nth, nz = MESH[:3]
+    n = nr * nth * nz
+    f0 = g.make_pcorr_fields(nr, nth, nz, seed=0)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def to_dev(f):
+        d = f.copy()
+        for k, v in list(d.__dict__.items()):
+            if isinstance(v, np.ndarray):
+                setattr(d, k, torch.from_numpy(v).cuda())
+        return d
+
+    with eaf.CGSolver(nr, nth, nz) as cg:
+        d = to_dev(f0)
+        for _ in range(args.warmup):
+            cg.pressure_correct(d, device_ptrs=True)
+        kms = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            cg.pressure_correct(d, device_ptrs=True)
+            kms += cg.last_timing()["kernel_ms"]
+        host = f0.copy()
+        e2e = 0.0
+        for _ in range(args.steps):
+            h = f0.copy()
+            cg.pressure_correct(h)
+            e2e += cg.last_timing()["e2e_ms"]
+        cg.pressure_correct(host)
+    import oracle
+    ref = f0.copy()
+    t0 = time.perf_counter()
+    oracle.pressure_correct(ref)
+    cpu_s = time.perf_counter() - t0
+    same = all(np.array_equal(a, ref.outputs()[k]) for k, a in host.outputs().items())
+    value = n * args.steps / (kms / 1e3)
+    achieved = PCORR_BYTES_PER_CELL * n * args.steps / (kms / 1e3) / 1e9
+    peak, kind = measured_peaks()
+    nh = (nr + 4) * (nth + 4) * (nz + 4)
+    line = _base_line("post-CG pressure corrections, cells/s (60x120x84, two phases)", value,
+                      "cells/s", args.steps, args.warmup, kms / args.steps,
+                      "flux export + velocity/pressure corrections + sealed cells",
+                      {"mesh": [nr, nth, nz], "cells": n, "phases": 2,
+                       "l2": "flushed between steps (256 MiB memset)"})
+    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": f"{kind} hbm_gbs",
+                        "algorithmic_bytes_per_cell": PCORR_BYTES_PER_CELL,
+                        "kernel": "pcorr_update_kernel + pcorr_sealed_kernel + pcorr_wrap_kernel"}
+    line["e2e"] = {"value": n * args.steps / (e2e / 1e3), "unit": "cells/s",
+                   "h2d_bytes_per_step": 26 * 8 * nh + 6 * 4 * nh,
+                   "d2h_bytes_per_step": 10 * 8 * nh + 3 * 4 * nh}
+    line["bitwise_equal_to_cpu"] = bool(same)
+    line["cpu_baseline"] = {"value": n / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+                            "sample": f"oracle port, one call, one thread, {cpu_s:.3f} s"}
+    line["gpu_launches"] = 3 * args.steps
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch(args):
     """96 uneven systems (40 at 12x24x16, 30 at 18x36x24, 20 at 35x70x50,
     6 at 60x120x84; seed = system id) in one persistent launch replayed from
@@ -620,7 +691,8 @@ def main(argv=None):
     ap.add_argument("--ref-iters", type=int, default=1500,
                     help="iteration cap per reference-arm step (bounded sample)")
     ap.add_argument("--tdma-sweeps", type=int, default=3)
-    ap.add_argument("--workload", choices=["production", "fine", "batch", "serve", "tdma"],
+    ap.add_argument("--workload", choices=["production", "fine", "batch", "serve", "tdma",
+                                           "pcorr"],
                     default="production")
     ap.add_argument("--mixed-outer", type=int, default=30)
     ap.add_argument("--mixed-inner", type=int, default=3000)
@@ -631,7 +703,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.workload != "production" and args.impl == "ours":
         return {"fine": run_fine, "batch": run_batch, "serve": run_serve,
-                "tdma": run_tdma}[args.workload](args)
+                "tdma": run_tdma, "pcorr": run_pcorr}[args.workload](args)
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local_rank = _env_int("LOCAL_RANK", 0)
