@@ -21,6 +21,10 @@
 ! radiation and continuity (e.g. src/mod_momentum_3d.f90:326-329):
 !     residual = compute_residual_3d_gpu(aW, ..., Su, vel, m)
 !     call tdma_3d_gpu(aW, ..., Su, vel, m, cfg%max_inner_mom)
+! and the post-CG corrections of solve_pressure_correction
+! (src/mod_pressure_3d.f90:333-397 with correct_velocities :689-746) become
+! one call of pressure_correct_gpu (fill an eaf_pcorr_fields with c_loc of
+! the arrays; see its comment).
 !===============================================================================
 module mod_solver_gpu
     use iso_c_binding
@@ -30,8 +34,25 @@ module mod_solver_gpu
     public :: tdma_3d_gpu, compute_residual_3d_gpu
     public :: eaf_cg_create, eaf_cg_destroy, eaf_cg_solve_f64, eaf_cg_solve_mixed
     public :: eaf_tdma_3d_f64, eaf_residual_3d_f64
+    public :: eaf_phase_fields, eaf_pcorr_fields, pressure_correct_gpu
 
     integer(c_int), parameter, public :: EAF_OK = 0, EAF_ENONFINITE = 3
+
+    ! Mirrors of eaf_phase_fields_t / eaf_pcorr_fields_t (include/eafcg.h):
+    ! c_loc of the phase and workspace arrays, c_null_ptr for the gas when
+    ! it is not in the pressure equation.
+    type, bind(C) :: eaf_phase_fields
+        type(c_ptr) :: alpha, aP_ur, aP_uth, aP_uz, ur, uth, uz
+    end type eaf_phase_fields
+
+    type, bind(C) :: eaf_pcorr_fields
+        type(c_ptr) :: pp, Fs_r, Fs_th, Fs_z, ac_r, ac_th, ac_z
+        type(c_ptr) :: Fc_r, Fc_th, Fc_z, vol, r, theta, z, p
+        type(eaf_phase_fields) :: liq, gas
+        type(c_ptr) :: lk_r, lk_th, lk_z, cell_type, act_l, act_g
+        integer(c_int) :: has_gas
+        real(c_double) :: alpha_p
+    end type eaf_pcorr_fields
 
     interface
         integer(c_int) function eaf_cg_create(h, nr, nth, nz, device) &
@@ -93,6 +114,13 @@ module mod_solver_gpu
             real(c_double), intent(in) :: phi(*)
             real(c_double), intent(out) :: residual
         end function eaf_residual_3d_f64
+
+        integer(c_int) function eaf_pressure_correct_f64(h, f) &
+                bind(C, name="eaf_pressure_correct_f64")
+            import :: c_int, c_ptr, eaf_pcorr_fields
+            type(c_ptr), value :: h
+            type(eaf_pcorr_fields), intent(in) :: f
+        end function eaf_pressure_correct_f64
     end interface
 
     ! One handle per mesh size, kept across SIMPLE iterations like the
@@ -206,6 +234,24 @@ contains
         if (st /= EAF_OK) error stop 'eaf_residual_3d_f64 failed'
         res = r
     end function compute_residual_3d_gpu
+
+    ! Replaces src/mod_pressure_3d.f90:333-397 (flux export, halo refresh of
+    ! the fluxes and link flags, correct_velocities of both phases, pressure
+    ! update and clamp, sealed cells, halo refresh of p): the caller fills
+    ! f with c_loc of sh%pp, Fs_*, ac_*, ws_Fc_*, m%vol, m%r, m%theta, m%z,
+    ! sh%p, the phase arrays (liq, gas), ws_Fc_lk_*, m%cell_type, act_l and
+    ! act_g (default logicals), has_gas and cfg%alpha_p. Bit-identical to the
+    ! serial Fortran. Serial meshes only.
+    subroutine pressure_correct_gpu(f, m)
+        use mod_types_3d, only: mesh_t
+        type(eaf_pcorr_fields), intent(in) :: f
+        type(mesh_t), intent(in) :: m
+        integer(c_int) :: st
+        if (m%is_parallel) error stop 'pressure_correct_gpu: decomposed meshes are not supported'
+        call ensure_handle(m%nr, m%ntheta, m%nz)
+        st = eaf_pressure_correct_f64(handle, f)
+        if (st /= EAF_OK) error stop 'eaf_pressure_correct_f64 failed'
+    end subroutine pressure_correct_gpu
 
     subroutine cg_gpu_release()
         integer(c_int) :: st
