@@ -75,6 +75,14 @@ SIGNATURES = [
     ("eaf_tdma_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _ci]),
     ("eaf_residual_3d_f64", _ci, [_vp] + _A8 + [_vp, _pd]),
     ("eaf_pressure_correct_f64", _ci, [_vp, _vp]),
+    ("eaf_mr_grid", _ci, [_ci, _ci, _ci, _ci, _pi]),
+    ("eaf_mr_block", _ci, [_ci, _ci, _ci, _pi, _pi, _pi, _pi]),
+    ("eaf_mr_pack_count", ctypes.c_longlong, [_pi, _pi, _pi]),
+    ("eaf_mr_unpack_count", ctypes.c_longlong, [_ci, _ci, _pi, _pi]),
+    ("eaf_mr_pack", _ci, [_vp, _pi, _pi, _pi, _vp]),
+    ("eaf_mr_place", _ci, [_vp, _ci, _ci, _ci, _pi, _pi, _pi, _pi, _vp]),
+    ("eaf_mr_extract", _ci, [_vp, _ci, _ci, _ci, _pi, _pi, _vp]),
+    ("eaf_mr_unpack", _ci, [_vp, _ci, _ci, _pi, _pi, _vp]),
     ("eaf_pressure_correct_f64_device", _ci, [_vp, _vp]),
     ("eaf_residual_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _pd]),
     ("eaf_cg_solve_mixed", _ci,

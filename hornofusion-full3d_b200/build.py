@@ -38,6 +38,7 @@ UNITS = {
     "diag.cu": [],
     "tdma.cu": ["-fmad=false"],
     "pcorr.cu": ["-fmad=false"],
+    "multirank.cu": [],
 }
 
 

@@ -212,6 +212,42 @@ int eaf_pressure_correct_f64(eaf_cg_t h, const eaf_pcorr_fields_t* f);
  * before return). */
 int eaf_pressure_correct_f64_device(eaf_cg_t h, const eaf_pcorr_fields_t* f);
 
+/* Multi-rank drop-in helpers (host-side index work, no device and no MPI):
+ * an MPI-decomposed run (m%is_parallel) gathers its blocks onto one rank,
+ * solves there on the GPU and scatters the solution back.
+ *   eaf_mr_grid   the npr x npth x npz process grid for nprocs ranks
+ *                 (factorize_3d, src/mod_mpi_topology.f90:157-204);
+ *   eaf_mr_block  a block's extents and 1-based global start from its
+ *                 Cartesian coordinates (decompose_domain, :209-250);
+ *   eaf_mr_pack   (every rank) its interior, plus the two halo layers
+ *                 beyond a physical r or z boundary it touches, of one local
+ *                 array (-1:iloc+2, -1:jloc+2, -1:kloc+2) into a buffer of
+ *                 eaf_mr_pack_count doubles;
+ *   eaf_mr_place  (solving rank) that buffer into the global halo-layout
+ *                 array (the gather_global_field pattern,
+ *                 src/mod_parallel_utils.f90:92-111);
+ *   eaf_mr_extract / eaf_mr_unpack  (solving rank / every rank) the block's
+ *                 cells whose global r and z index lies in the domain (theta
+ *                 periodic) -- interior and the halos that the final
+ *                 26-neighbour exchange of cg_3d_mpi (:567) fills; halos beyond
+ *                 a physical boundary keep their values -- eaf_mr_unpack_count
+ *                 doubles.
+ * grid, coords, loc and start are 3-vectors in (r, theta, z) order. */
+int eaf_mr_grid(int nprocs, int nr, int nth, int nz, int grid[3]);
+int eaf_mr_block(int nr, int nth, int nz, const int grid[3], const int coords[3], int loc[3],
+                 int start[3]);
+long long eaf_mr_pack_count(const int grid[3], const int coords[3], const int loc[3]);
+long long eaf_mr_unpack_count(int nr, int nz, const int start[3], const int loc[3]);
+int eaf_mr_pack(const double* local, const int grid[3], const int coords[3],
+                const int loc[3], double* buf);
+int eaf_mr_place(double* global, int nr, int nth, int nz, const int grid[3],
+                 const int coords[3], const int loc[3], const int start[3],
+                 const double* buf);
+int eaf_mr_extract(const double* global, int nr, int nth, int nz, const int loc[3],
+                   const int start[3], double* buf);
+int eaf_mr_unpack(double* local, int nr, int nz, const int loc[3], const int start[3],
+                  const double* buf);
+
 /* Bound on every device-side barrier wait, in milliseconds (default 2000). */
 int eaf_cg_set_timeout_ms(eaf_cg_t h, double ms);
 
