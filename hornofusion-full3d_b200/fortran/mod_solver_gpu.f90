@@ -35,6 +35,7 @@ module mod_solver_gpu
     public :: eaf_cg_create, eaf_cg_destroy, eaf_cg_solve_f64, eaf_cg_solve_mixed
     public :: eaf_tdma_3d_f64, eaf_residual_3d_f64
     public :: eaf_phase_fields, eaf_pcorr_fields, pressure_correct_gpu
+    public :: cg_3d_gpu_mpi
 
     integer(c_int), parameter, public :: EAF_OK = 0, EAF_ENONFINITE = 3
 
@@ -114,6 +115,62 @@ module mod_solver_gpu
             real(c_double), intent(in) :: phi(*)
             real(c_double), intent(out) :: residual
         end function eaf_residual_3d_f64
+
+        integer(c_int) function eaf_mr_block(nr, nth, nz, grid, coords, loc, start) &
+                bind(C, name="eaf_mr_block")
+            import :: c_int
+            integer(c_int), value :: nr, nth, nz
+            integer(c_int), intent(in) :: grid(3), coords(3)
+            integer(c_int), intent(out) :: loc(3), start(3)
+        end function eaf_mr_block
+
+        integer(c_long_long) function eaf_mr_pack_count(grid, coords, loc) &
+                bind(C, name="eaf_mr_pack_count")
+            import :: c_int, c_long_long
+            integer(c_int), intent(in) :: grid(3), coords(3), loc(3)
+        end function eaf_mr_pack_count
+
+        integer(c_long_long) function eaf_mr_unpack_count(nr, nz, start, loc) &
+                bind(C, name="eaf_mr_unpack_count")
+            import :: c_int, c_long_long
+            integer(c_int), value :: nr, nz
+            integer(c_int), intent(in) :: start(3), loc(3)
+        end function eaf_mr_unpack_count
+
+        integer(c_int) function eaf_mr_pack(local, grid, coords, loc, buf) &
+                bind(C, name="eaf_mr_pack")
+            import :: c_int, c_double
+            real(c_double), intent(in) :: local(*)
+            integer(c_int), intent(in) :: grid(3), coords(3), loc(3)
+            real(c_double), intent(out) :: buf(*)
+        end function eaf_mr_pack
+
+        integer(c_int) function eaf_mr_place(global, nr, nth, nz, grid, coords, loc, &
+                start, buf) bind(C, name="eaf_mr_place")
+            import :: c_int, c_double
+            real(c_double), intent(inout) :: global(*)
+            integer(c_int), value :: nr, nth, nz
+            integer(c_int), intent(in) :: grid(3), coords(3), loc(3), start(3)
+            real(c_double), intent(in) :: buf(*)
+        end function eaf_mr_place
+
+        integer(c_int) function eaf_mr_extract(global, nr, nth, nz, loc, start, buf) &
+                bind(C, name="eaf_mr_extract")
+            import :: c_int, c_double
+            real(c_double), intent(in) :: global(*)
+            integer(c_int), value :: nr, nth, nz
+            integer(c_int), intent(in) :: loc(3), start(3)
+            real(c_double), intent(out) :: buf(*)
+        end function eaf_mr_extract
+
+        integer(c_int) function eaf_mr_unpack(local, nr, nz, loc, start, buf) &
+                bind(C, name="eaf_mr_unpack")
+            import :: c_int, c_double
+            real(c_double), intent(inout) :: local(*)
+            integer(c_int), value :: nr, nz
+            integer(c_int), intent(in) :: loc(3), start(3)
+            real(c_double), intent(in) :: buf(*)
+        end function eaf_mr_unpack
 
         integer(c_int) function eaf_pressure_correct_f64(h, f) &
                 bind(C, name="eaf_pressure_correct_f64")
@@ -252,6 +309,119 @@ contains
         st = eaf_pressure_correct_f64(handle, f)
         if (st /= EAF_OK) error stop 'eaf_pressure_correct_f64 failed'
     end subroutine pressure_correct_gpu
+
+    ! Same dummies as cg_3d_mpi for DECOMPOSED meshes (m%is_parallel): the
+    ! blocks of the eight coefficient arrays and phi are gathered onto rank 0
+    ! of m%topo%comm_cart, solved there on the GPU as one global system, and
+    ! each rank gets back its block of the solution with every halo cell
+    ! inside the domain filled (what cg_3d_mpi's closing halo exchange fills,
+    ! src/mod_solver_3d.f90:567); residual and n_iter are broadcast. The
+    ! answer is the serial solve's (the parallel reference associates its dot
+    ! products per rank). Rank 0 must see a GPU.
+    subroutine cg_3d_gpu_mpi(aW, aE, aS, aN, aB, aT, aP, Su, phi, m, &
+                             max_iter, tol, residual, n_iter)
+        use mpi
+        use mod_constants, only: dp
+        use mod_types_3d, only: mesh_t
+        real(dp), intent(in), contiguous  :: aW(-1:,-1:,-1:), aE(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aS(-1:,-1:,-1:), aN(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aB(-1:,-1:,-1:), aT(-1:,-1:,-1:)
+        real(dp), intent(in), contiguous  :: aP(-1:,-1:,-1:), Su(-1:,-1:,-1:)
+        real(dp), intent(inout), contiguous :: phi(-1:,-1:,-1:)
+        type(mesh_t), intent(in) :: m
+        integer, intent(in)      :: max_iter
+        real(dp), intent(in)     :: tol
+        real(dp), intent(out)    :: residual
+        integer, intent(out)     :: n_iter
+        integer(c_int) :: grid(3), coords(3), loc(3), start(3), st, nit, p
+        integer(c_int), allocatable :: allc(:,:)
+        integer(c_long_long) :: np1, nu
+        integer :: ierr, nprocs, rank, a, nrg, nthg, nzg
+        integer, allocatable :: cnt(:), dsp(:), ucnt(:), udsp(:)
+        real(c_double), allocatable :: sbuf(:), gbuf(:), glob(:,:), ubuf(:)
+        real(c_double) :: res
+        real(c_double) :: outv(2)
+        ! global extents (m%nr and friends are the local block in a parallel run)
+        nrg = m%topo%nr_global; nthg = m%topo%nth_global; nzg = m%topo%nz_global
+        call MPI_Comm_size(m%topo%comm_cart, nprocs, ierr)
+        call MPI_Comm_rank(m%topo%comm_cart, rank, ierr)
+        grid = [m%topo%npr, m%topo%npth, m%topo%npz]
+        coords = m%topo%coords
+        loc = [m%topo%iloc, m%topo%jloc, m%topo%kloc]
+        start = [m%topo%iglobal_start, m%topo%jglobal_start, m%topo%kglobal_start]
+        np1 = eaf_mr_pack_count(grid, coords, loc)
+        allocate(sbuf(9 * np1))
+        st = eaf_mr_pack(aW, grid, coords, loc, sbuf(0*np1+1:))
+        st = eaf_mr_pack(aE, grid, coords, loc, sbuf(1*np1+1:))
+        st = eaf_mr_pack(aS, grid, coords, loc, sbuf(2*np1+1:))
+        st = eaf_mr_pack(aN, grid, coords, loc, sbuf(3*np1+1:))
+        st = eaf_mr_pack(aB, grid, coords, loc, sbuf(4*np1+1:))
+        st = eaf_mr_pack(aT, grid, coords, loc, sbuf(5*np1+1:))
+        st = eaf_mr_pack(aP, grid, coords, loc, sbuf(6*np1+1:))
+        st = eaf_mr_pack(Su, grid, coords, loc, sbuf(7*np1+1:))
+        st = eaf_mr_pack(phi, grid, coords, loc, sbuf(8*np1+1:))
+        allocate(allc(3, 0:nprocs-1), cnt(0:nprocs-1), dsp(0:nprocs-1))
+        allocate(ucnt(0:nprocs-1), udsp(0:nprocs-1))
+        call MPI_Gather(coords, 3, MPI_INTEGER, allc, 3, MPI_INTEGER, 0, &
+                        m%topo%comm_cart, ierr)
+        call MPI_Gather(int(9 * np1), 1, MPI_INTEGER, cnt, 1, MPI_INTEGER, 0, &
+                        m%topo%comm_cart, ierr)
+        if (rank == 0) then
+            dsp(0) = 0
+            do p = 1, nprocs - 1
+                dsp(p) = dsp(p-1) + cnt(p-1)
+            end do
+            allocate(gbuf(sum(cnt)))
+        else
+            allocate(gbuf(1))
+        end if
+        call MPI_Gatherv(sbuf, int(9 * np1), MPI_DOUBLE_PRECISION, gbuf, cnt, dsp, &
+                         MPI_DOUBLE_PRECISION, 0, m%topo%comm_cart, ierr)
+        if (rank == 0) then
+            allocate(glob((nrg+4)*(nthg+4)*(nzg+4), 9))
+            glob = 0.0_c_double
+            do p = 0, nprocs - 1
+                st = eaf_mr_block(nrg, nthg, nzg, grid, allc(:, p), loc, start)
+                np1 = cnt(p) / 9
+                do a = 1, 9
+                    st = eaf_mr_place(glob(:, a), nrg, nthg, nzg, grid, allc(:, p), loc, &
+                                      start, gbuf(dsp(p) + (a-1)*np1 + 1:))
+                end do
+            end do
+            call ensure_handle(nrg, nthg, nzg)
+            st = eaf_cg_solve_f64(handle, glob(:,1), glob(:,2), glob(:,3), glob(:,4), &
+                                  glob(:,5), glob(:,6), glob(:,7), glob(:,8), glob(:,9), &
+                                  int(max_iter, c_int), real(tol, c_double), res, nit)
+            if (st /= EAF_OK .and. st /= EAF_ENONFINITE) error stop 'eaf_cg_solve_f64 failed'
+            outv = [res, real(nit, c_double)]
+            do p = 0, nprocs - 1
+                st = eaf_mr_block(nrg, nthg, nzg, grid, allc(:, p), loc, start)
+                ucnt(p) = int(eaf_mr_unpack_count(nrg, nzg, start, loc))
+            end do
+            udsp(0) = 0
+            do p = 1, nprocs - 1
+                udsp(p) = udsp(p-1) + ucnt(p-1)
+            end do
+            allocate(ubuf(sum(ucnt)))
+            do p = 0, nprocs - 1
+                st = eaf_mr_block(nrg, nthg, nzg, grid, allc(:, p), loc, start)
+                st = eaf_mr_extract(glob(:, 9), nrg, nthg, nzg, loc, start, ubuf(udsp(p)+1:))
+            end do
+        else
+            allocate(ubuf(1))
+        end if
+        loc = [m%topo%iloc, m%topo%jloc, m%topo%kloc]
+        start = [m%topo%iglobal_start, m%topo%jglobal_start, m%topo%kglobal_start]
+        nu = eaf_mr_unpack_count(nrg, nzg, start, loc)
+        deallocate(sbuf)
+        allocate(sbuf(nu))
+        call MPI_Scatterv(ubuf, ucnt, udsp, MPI_DOUBLE_PRECISION, sbuf, int(nu), &
+                          MPI_DOUBLE_PRECISION, 0, m%topo%comm_cart, ierr)
+        st = eaf_mr_unpack(phi, nrg, nzg, loc, start, sbuf)
+        call MPI_Bcast(outv, 2, MPI_DOUBLE_PRECISION, 0, m%topo%comm_cart, ierr)
+        residual = outv(1)
+        n_iter = int(outv(2))
+    end subroutine cg_3d_gpu_mpi
 
     subroutine cg_gpu_release()
         integer(c_int) :: st
