@@ -561,6 +561,86 @@ def run_pcorr(args):
     return 0
 
 
+# flags 7 (liquid room, gas in the equation, gas compressibility): reads 24
+# doubles (vol, Ar, Ath, Az, p, liq_room, 8 + 8 phase arrays, liq_T, gas
+# T_old) and 4 ints (cell type, outlet, activity masks), writes 18 doubles
+# (coefficients, Su, pp, Fs/ac/Fc) and 3 ints (link flags), each once per
+# halo-layout element.
+ASSEMBLY_BYTES_PER_ELEM = 24 * 8 + 4 * 4 + 18 * 8 + 3 * 4
+
+
+def run_assemble(args):
+    """Assembly of the pressure-correction equation (solve_pressure_correction
+    up to the CG) on the 60x120x84 mesh with both phases and every switch on,
+    fields resident on the device (value, HBM roofline) and through the
+    host-pointer entry (e2e); the single-thread CPU restatement as baseline."""
+    import numpy as np
+    import torch
+    eaf = importlib.import_module(PKG)
+    g = importlib.import_module(PKG + ".eafgen")
+    nr, nth, nz = MESH[:3]
+    n = nr * nth * nz
+    nh = (nr + 4) * (nth + 4) * (nz + 4)
+    f0 = g.make_assembly_fields(nr, nth, nz, seed=0, flags=7)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def to_dev(f):
+        d = f.copy()
+        for k, v in list(d.__dict__.items()):
+            if isinstance(v, np.ndarray):
+                setattr(d, k, torch.from_numpy(v).cuda())
+        return d
+
+    with eaf.CGSolver(nr, nth, nz) as cg:
+        d = to_dev(f0)
+        for _ in range(args.warmup):
+            cg.pressure_assemble(d, device_ptrs=True)
+        kms = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            cg.pressure_assemble(d, device_ptrs=True)
+            kms += cg.last_timing()["kernel_ms"]
+        host = f0.copy()
+        e2e = 0.0
+        for _ in range(args.steps):
+            h = f0.copy()
+            cg.pressure_assemble(h)
+            e2e += cg.last_timing()["e2e_ms"]
+        res = cg.pressure_assemble(host)
+    import oracle
+    ref = f0.copy()
+    t0 = time.perf_counter()
+    res_ref = oracle.pressure_assemble(ref)
+    cpu_s = time.perf_counter() - t0
+    same = all(np.array_equal(a, ref.outputs()[k]) for k, a in host.outputs().items())
+    value = n * args.steps / (kms / 1e3)
+    achieved = ASSEMBLY_BYTES_PER_ELEM * nh * args.steps / (kms / 1e3) / 1e9
+    peak, kind = measured_peaks()
+    line = _base_line("pressure-equation assembly, cells/s (60x120x84, two phases)", value,
+                      "cells/s", args.steps, args.warmup, kms / args.steps,
+                      "gradients + liquid/gas Rhie-Chow faces + compressibility + "
+                      "diagonal + boundary folding + continuity residual",
+                      {"mesh": [nr, nth, nz], "cells": n, "phases": 2, "flags": 7,
+                       "l2": "flushed between steps (256 MiB memset)"})
+    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": f"{kind} hbm_gbs",
+                        "algorithmic_bytes_per_halo_element": ASSEMBLY_BYTES_PER_ELEM,
+                        "kernel": "asm_gradient_kernel + asm_face_kernel + "
+                                  "asm_residual_kernel"}
+    line["e2e"] = {"value": n * args.steps / (e2e / 1e3), "unit": "cells/s",
+                   "h2d_bytes_per_step": 24 * 8 * nh + 4 * 4 * nh
+                   + 8 * (nr + nth + nz + 12),
+                   "d2h_bytes_per_step": 18 * 8 * nh + 3 * 4 * nh + 8}
+    line["bitwise_equal_to_cpu"] = bool(same)
+    line["residual_rel_diff"] = abs(res - res_ref) / abs(res_ref)
+    line["cpu_baseline"] = {"value": n / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+                            "sample": f"oracle port, one call, one thread, {cpu_s:.3f} s"}
+    line["gpu_launches"] = 3 * args.steps
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch(args):
     """96 uneven systems (40 at 12x24x16, 30 at 18x36x24, 20 at 35x70x50,
     6 at 60x120x84; seed = system id) in one persistent launch replayed from
@@ -692,7 +772,7 @@ def main(argv=None):
                     help="iteration cap per reference-arm step (bounded sample)")
     ap.add_argument("--tdma-sweeps", type=int, default=3)
     ap.add_argument("--workload", choices=["production", "fine", "batch", "serve", "tdma",
-                                           "pcorr"],
+                                           "pcorr", "assemble"],
                     default="production")
     ap.add_argument("--mixed-outer", type=int, default=30)
     ap.add_argument("--mixed-inner", type=int, default=3000)
@@ -703,7 +783,8 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.workload != "production" and args.impl == "ours":
         return {"fine": run_fine, "batch": run_batch, "serve": run_serve,
-                "tdma": run_tdma, "pcorr": run_pcorr}[args.workload](args)
+                "tdma": run_tdma, "pcorr": run_pcorr,
+                "assemble": run_assemble}[args.workload](args)
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local_rank = _env_int("LOCAL_RANK", 0)

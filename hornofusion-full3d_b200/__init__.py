@@ -163,6 +163,50 @@ class CGSolver:
               else self._lib.eaf_pressure_correct_f64)
         check(fn(self._h, ctypes.byref(c)), "eaf_pressure_correct_f64")
 
+    def pressure_assemble(self, fields, device_ptrs: bool = False) -> float:
+        """Assembly of the pressure-correction equation (solve_pressure_correction
+        up to the CG, src/mod_pressure_3d.f90:135-310, with apply_pressure_bc,
+        src/mod_boundary_3d.f90:180-277) into the output arrays of ``fields``
+        (an object with the attributes of eafgen.AssemblyFields: float64
+        halo-layout arrays, int32 masks, coordinate arrays, ``flags`` -- 1
+        liquid room valid, 2 gas in the equation, 4 gas compressibility -- and
+        ``scalars`` = (dt, rho_gas, T_ambient, beta_expansion)). Returns the
+        continuity residual sum|Su| / flux_ref."""
+        from ._lib import ASSEMBLY_IN, ASSEMBLY_OUT, AssemblyFieldsC, PhaseState
+
+        ints = ("cell_type", "outlet", "act_l", "act_g", "lk_r", "lk_th", "lk_z")
+
+        def addr(name, a):
+            if a is None:
+                return None
+            if isinstance(a, np.ndarray):
+                want = np.int32 if name in ints else np.float64
+                if a.dtype != want or not a.flags.c_contiguous:
+                    raise ValueError(f"{name} must be C-contiguous {np.dtype(want)}")
+                return a.ctypes.data
+            if hasattr(a, "data_ptr"):
+                return a.data_ptr()
+            raise TypeError(f"unsupported array type {type(a)!r}")
+
+        c = AssemblyFieldsC()
+        for n in ASSEMBLY_IN + ASSEMBLY_OUT:
+            setattr(c, n, addr(n, getattr(fields, n, None)))
+        for ph in ("liq", "gas"):
+            setattr(c, ph, PhaseState(*[addr(n, getattr(fields, ph + "_" + n, None)) for n in
+                                        ("alpha", "rho", "ur", "uth", "uz", "aP_ur",
+                                         "aP_uth", "aP_uz")]))
+        c.liq_T = addr("liq_T", getattr(fields, "liq_T", None))
+        c.gas_T_old = addr("gas_T_old", getattr(fields, "gas_T_old", None))
+        fl = int(fields.flags)
+        c.liq_room_valid, c.gas_in_poisson, c.gas_compressibility = \
+            fl & 1, (fl >> 1) & 1, (fl >> 2) & 1
+        c.dt, c.rho_gas, c.T_ambient, c.beta_expansion = [float(x) for x in fields.scalars]
+        res = ctypes.c_double()
+        fn = (self._lib.eaf_pressure_assemble_f64_device if device_ptrs
+              else self._lib.eaf_pressure_assemble_f64)
+        check(fn(self._h, ctypes.byref(c), ctypes.byref(res)), "eaf_pressure_assemble_f64")
+        return res.value
+
     def solve_mixed(self, arrays, phi, tol: float = SOR_TOL_PRESSURE,
                     inner_tol: float = 0.1, max_outer: int = 200,
                     max_inner: int = 100000, device_ptrs: bool = False):

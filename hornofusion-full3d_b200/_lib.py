@@ -50,6 +50,31 @@ class PcorrFieldsC(ctypes.Structure):
                 + [("has_gas", ctypes.c_int), ("alpha_p", ctypes.c_double)])
 
 
+class PhaseState(ctypes.Structure):
+    """eaf_phase_state_t"""
+    _fields_ = [(n, ctypes.c_void_p) for n in
+                ("alpha", "rho", "ur", "uth", "uz", "aP_ur", "aP_uth", "aP_uz")]
+
+
+ASSEMBLY_IN = ("cell_type", "outlet", "act_l", "act_g", "vol", "Ar", "Ath", "Az",
+               "r", "theta", "z", "p", "liq_room")
+ASSEMBLY_OUT = ("aW", "aE", "aS", "aN", "aB", "aT", "aP", "Su", "pp", "Fs_r", "Fs_th",
+                "Fs_z", "ac_r", "ac_th", "ac_z", "Fc_r", "Fc_th", "Fc_z",
+                "lk_r", "lk_th", "lk_z")
+
+
+class AssemblyFieldsC(ctypes.Structure):
+    """eaf_assembly_fields_t"""
+    _fields_ = ([(n, ctypes.c_void_p) for n in ASSEMBLY_IN]
+                + [("liq", PhaseState), ("gas", PhaseState)]
+                + [("liq_T", ctypes.c_void_p), ("gas_T_old", ctypes.c_void_p)]
+                + [(n, ctypes.c_int) for n in
+                   ("liq_room_valid", "gas_in_poisson", "gas_compressibility")]
+                + [(n, ctypes.c_double) for n in
+                   ("dt", "rho_gas", "T_ambient", "beta_expansion")]
+                + [(n, ctypes.c_void_p) for n in ASSEMBLY_OUT])
+
+
 STATUS_NAMES = {
     0: "EAF_OK", 1: "EAF_ECUDA", 2: "EAF_EINVAL", 3: "EAF_ENONFINITE",
     4: "EAF_ETIMEOUT", 5: "EAF_EUNSUPPORTED", 6: "EAF_ENOMEM", 7: "EAF_EADMIT",
@@ -84,6 +109,8 @@ SIGNATURES = [
     ("eaf_mr_extract", _ci, [_vp, _ci, _ci, _ci, _pi, _pi, _vp]),
     ("eaf_mr_unpack", _ci, [_vp, _ci, _ci, _pi, _pi, _vp]),
     ("eaf_pressure_correct_f64_device", _ci, [_vp, _vp]),
+    ("eaf_pressure_assemble_f64", _ci, [_vp, _vp, _pd]),
+    ("eaf_pressure_assemble_f64_device", _ci, [_vp, _vp, _pd]),
     ("eaf_residual_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _pd]),
     ("eaf_cg_solve_mixed", _ci,
      [_vp] + _A8 + [_vp, _ci, _ci, _cd, _cd, _pd, _pi, _pi]),

@@ -39,6 +39,7 @@ UNITS = {
     "tdma.cu": ["-fmad=false"],
     "pcorr.cu": ["-fmad=false"],
     "multirank.cu": [],
+    "assemble.cu": ["-fmad=false"],
 }
 
 

@@ -50,6 +50,9 @@ struct eaf_cg {
   double* tdma_fac;  // TDMA line factors (lazy)
   double* pc_d;      // post-CG correction mirror: doubles (lazy)
   int* pc_i;         // post-CG correction mirror: ints (lazy)
+  double* asm_d;     // assembly mirror: doubles (lazy)
+  int* asm_i;        // assembly mirror: ints (lazy)
+  double* asm_s;     // assembly scratch: gradients, partials, residual (lazy)
 };
 
 namespace eaf {
@@ -103,6 +106,9 @@ static void free_handle(eaf_cg* h) {
   cudaFree(h->tdma_fac);
   cudaFree(h->pc_d);
   cudaFree(h->pc_i);
+  cudaFree(h->asm_d);
+  cudaFree(h->asm_i);
+  cudaFree(h->asm_s);
   if (h->res_h) cudaFreeHost(h->res_h);
   for (int i = 0; i < 6; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -525,6 +531,68 @@ int run_pcorr(eaf_cg* h, const eaf_pcorr_fields_t& f) {
   return EAF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Pressure-equation assembly.
+// ---------------------------------------------------------------------------
+constexpr int kAsmIn = 24;   // halo double inputs of the mirror
+constexpr int kAsmOut = 18;  // halo double outputs
+constexpr int kAsmInts = 7;
+
+bool assembly_fields_ok(const eaf_assembly_fields_t* f) {
+  if (!f || !(f->dt > 0.0)) return false;
+  const void* req[] = {f->cell_type, f->outlet, f->act_l, f->act_g, f->vol, f->Ar, f->Ath,
+                       f->Az, f->r, f->theta, f->z, f->p,
+                       f->liq.alpha, f->liq.rho, f->liq.ur, f->liq.uth, f->liq.uz,
+                       f->liq.aP_ur, f->liq.aP_uth, f->liq.aP_uz,
+                       f->aW, f->aE, f->aS, f->aN, f->aB, f->aT, f->aP, f->Su, f->pp,
+                       f->Fs_r, f->Fs_th, f->Fs_z, f->ac_r, f->ac_th, f->ac_z,
+                       f->Fc_r, f->Fc_th, f->Fc_z, f->lk_r, f->lk_th, f->lk_z};
+  for (const void* q : req)
+    if (!q) return false;
+  if (f->liq_room_valid && !f->liq_room) return false;
+  if (f->gas_in_poisson) {
+    const void* gas[] = {f->liq_T, f->gas.alpha, f->gas.rho, f->gas.ur, f->gas.uth,
+                         f->gas.uz, f->gas.aP_ur, f->gas.aP_uth, f->gas.aP_uz};
+    for (const void* q : gas)
+      if (!q) return false;
+  }
+  if (f->gas_compressibility && (!f->gas.alpha || !f->gas.rho || !f->gas_T_old)) return false;
+  return true;
+}
+
+// Fields the kernels never read are cleared, so a flag that is off cannot
+// lead them to a stale pointer.
+eaf_assembly_fields_t assembly_normalised(const eaf_assembly_fields_t& f) {
+  eaf_assembly_fields_t d = f;
+  d.liq_room_valid = f.liq_room_valid ? 1 : 0;
+  d.gas_in_poisson = f.gas_in_poisson ? 1 : 0;
+  d.gas_compressibility = f.gas_compressibility ? 1 : 0;
+  if (!d.liq_room_valid) d.liq_room = nullptr;
+  if (!d.gas_in_poisson) {
+    d.liq_T = nullptr;
+    d.gas.ur = d.gas.uth = d.gas.uz = nullptr;
+    d.gas.aP_ur = d.gas.aP_uth = d.gas.aP_uz = nullptr;
+    if (!d.gas_compressibility) d.gas.alpha = d.gas.rho = nullptr;
+  }
+  if (!d.gas_compressibility) d.gas_T_old = nullptr;
+  return d;
+}
+
+int run_assemble(eaf_cg* h, const eaf_assembly_fields_t& f) {
+  if (!h->asm_s) {
+    EAF_CUDA(cudaMalloc((void**)&h->asm_s,
+                        sizeof(double) * eaf::assembly_scratch_doubles(h->nr, h->nth, h->nz)));
+  }
+  EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
+  EAF_CUDA(eaf::launch_assemble_f64(f, h->nr, h->nth, h->nz, h->asm_s, h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[3], h->st));
+  EAF_CUDA(cudaMemcpyAsync(&h->res_h->residual,
+                           eaf::assembly_result(h->asm_s, h->nr, h->nth, h->nz),
+                           sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  h->last_kernels = 3;
+  return EAF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -746,6 +814,104 @@ int eaf_pressure_correct_f64(eaf_cg_t h, const eaf_pcorr_fields_t* f) {
                              cudaMemcpyDeviceToHost, h->st));
   EAF_CUDA(cudaEventRecord(h->ev[5], h->st));
   EAF_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
+  if (cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]) == cudaSuccess) h->last_e2e_ms = ms;
+  return EAF_OK;
+}
+
+int eaf_pressure_assemble_f64_device(eaf_cg_t h, const eaf_assembly_fields_t* f,
+                                     double* residual) {
+  if (!h || !residual || !assembly_fields_ok(f)) return EAF_EINVAL;
+  if (h->nh > (size_t)INT32_MAX) return EAF_EUNSUPPORTED;  // 32-bit element indices
+  eaf::DeviceGuard guard(h->device);
+  const eaf_assembly_fields_t d = assembly_normalised(*f);
+  int rc = run_assemble(h, d);
+  if (rc != EAF_OK) return rc;
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  *residual = h->res_h->residual;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
+  return EAF_OK;
+}
+
+int eaf_pressure_assemble_f64(eaf_cg_t h, const eaf_assembly_fields_t* f, double* residual) {
+  if (!h || !residual || !assembly_fields_ok(f)) return EAF_EINVAL;
+  if (h->nh > (size_t)INT32_MAX) return EAF_EUNSUPPORTED;  // 32-bit element indices
+  eaf::DeviceGuard guard(h->device);
+  const size_t nh = h->nh;
+  const size_t nc = (size_t)(h->nr + 4) + (h->nth + 4) + (h->nz + 4);
+  if (!h->asm_d) {
+    EAF_CUDA(cudaMalloc((void**)&h->asm_d, sizeof(double) * ((kAsmIn + kAsmOut) * nh + nc)));
+  }
+  if (!h->asm_i) {
+    EAF_CUDA(cudaMalloc((void**)&h->asm_i, sizeof(int) * kAsmInts * nh));
+  }
+  const eaf_assembly_fields_t src = assembly_normalised(*f);
+  eaf_assembly_fields_t d = src;
+  auto slot = [&](int i) { return h->asm_d + (size_t)i * nh; };
+  // mirror slots: 0 vol, 1-3 Ar Ath Az, 4 p, 5 liq_room, 6-13 liquid state,
+  // 14 liq_T, 15-22 gas state, 23 gas_T_old, 24-41 outputs (aW .. Fc_z)
+  const double* in[kAsmIn] = {src.vol, src.Ar, src.Ath, src.Az, src.p, src.liq_room,
+                              src.liq.alpha, src.liq.rho, src.liq.ur, src.liq.uth,
+                              src.liq.uz, src.liq.aP_ur, src.liq.aP_uth, src.liq.aP_uz,
+                              src.liq_T,
+                              src.gas.alpha, src.gas.rho, src.gas.ur, src.gas.uth,
+                              src.gas.uz, src.gas.aP_ur, src.gas.aP_uth, src.gas.aP_uz,
+                              src.gas_T_old};
+  const double** din[kAsmIn] = {&d.vol, &d.Ar, &d.Ath, &d.Az, &d.p, &d.liq_room,
+                                &d.liq.alpha, &d.liq.rho, &d.liq.ur, &d.liq.uth,
+                                &d.liq.uz, &d.liq.aP_ur, &d.liq.aP_uth, &d.liq.aP_uz,
+                                &d.liq_T,
+                                &d.gas.alpha, &d.gas.rho, &d.gas.ur, &d.gas.uth,
+                                &d.gas.uz, &d.gas.aP_ur, &d.gas.aP_uth, &d.gas.aP_uz,
+                                &d.gas_T_old};
+  EAF_CUDA(cudaEventRecord(h->ev[0], h->st));
+  for (int i = 0; i < kAsmIn; ++i) {
+    if (!in[i]) continue;  // not read under these flags
+    EAF_CUDA(cudaMemcpyAsync(slot(i), in[i], nh * sizeof(double), cudaMemcpyHostToDevice,
+                             h->st));
+    *din[i] = slot(i);
+  }
+  double* coords = slot(kAsmIn + kAsmOut);
+  EAF_CUDA(cudaMemcpyAsync(coords, src.r, (h->nr + 4) * sizeof(double),
+                           cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4, src.theta, (h->nth + 4) * sizeof(double),
+                           cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4 + h->nth + 4, src.z,
+                           (h->nz + 4) * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  d.r = coords;
+  d.theta = coords + h->nr + 4;
+  d.z = coords + h->nr + 4 + h->nth + 4;
+  const int* in_i[4] = {src.cell_type, src.outlet, src.act_l, src.act_g};
+  const int** din_i[4] = {&d.cell_type, &d.outlet, &d.act_l, &d.act_g};
+  for (int i = 0; i < 4; ++i) {
+    EAF_CUDA(cudaMemcpyAsync(h->asm_i + (size_t)i * nh, in_i[i], nh * sizeof(int),
+                             cudaMemcpyHostToDevice, h->st));
+    *din_i[i] = h->asm_i + (size_t)i * nh;
+  }
+  double* out_h[kAsmOut] = {src.aW, src.aE, src.aS, src.aN, src.aB, src.aT, src.aP,
+                            src.Su, src.pp, src.Fs_r, src.Fs_th, src.Fs_z,
+                            src.ac_r, src.ac_th, src.ac_z, src.Fc_r, src.Fc_th, src.Fc_z};
+  double** dout[kAsmOut] = {&d.aW, &d.aE, &d.aS, &d.aN, &d.aB, &d.aT, &d.aP, &d.Su, &d.pp,
+                            &d.Fs_r, &d.Fs_th, &d.Fs_z, &d.ac_r, &d.ac_th, &d.ac_z,
+                            &d.Fc_r, &d.Fc_th, &d.Fc_z};
+  for (int i = 0; i < kAsmOut; ++i) *dout[i] = slot(kAsmIn + i);
+  d.lk_r = h->asm_i + 4 * nh;
+  d.lk_th = h->asm_i + 5 * nh;
+  d.lk_z = h->asm_i + 6 * nh;
+  int rc = run_assemble(h, d);
+  if (rc != EAF_OK) return rc;
+  for (int i = 0; i < kAsmOut; ++i)
+    EAF_CUDA(cudaMemcpyAsync(out_h[i], *dout[i], nh * sizeof(double), cudaMemcpyDeviceToHost,
+                             h->st));
+  int* lk_h[3] = {src.lk_r, src.lk_th, src.lk_z};
+  for (int i = 0; i < 3; ++i)
+    EAF_CUDA(cudaMemcpyAsync(lk_h[i], h->asm_i + (size_t)(4 + i) * nh, nh * sizeof(int),
+                             cudaMemcpyDeviceToHost, h->st));
+  EAF_CUDA(cudaEventRecord(h->ev[5], h->st));
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  *residual = h->res_h->residual;
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
   if (cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]) == cudaSuccess) h->last_e2e_ms = ms;

@@ -153,6 +153,15 @@ cudaError_t run_div_check(long long n, unsigned long long seed, unsigned long lo
 cudaError_t launch_pcorr_f64(const eaf_pcorr_fields_t& f, int nr, int nth, int nz,
                              cudaStream_t st);
 
+// Pressure-equation assembly (solve_pressure_correction before the CG), three
+// launches on `st` into device pointers of `f`; `scratch` holds
+// assembly_scratch_doubles() doubles (gradients, block partials, and the
+// residual at assembly_result()).
+size_t assembly_scratch_doubles(int nr, int nth, int nz);
+cudaError_t launch_assemble_f64(const eaf_assembly_fields_t& f, int nr, int nth, int nz,
+                                double* scratch, cudaStream_t st);
+const double* assembly_result(double* scratch, int nr, int nth, int nz);
+
 // Threads per block of the batched kernels (FP64 and mixed).
 constexpr int kBatchBlock = 512;
 const void* batch_mixed_kernel_ptr();

@@ -414,6 +414,93 @@ def make_pcorr_fields(nr: int, nth: int, nz: int, seed: int = 0, has_gas: bool =
     return f
 
 
+# Assembly of the pressure-correction equation (solve_pressure_correction
+# before the CG): ordered like the oracle's arrays.
+ASM_DOUBLES_IN = ("vol", "Ar", "Ath", "Az", "r", "theta", "z", "p", "liq_room")
+ASM_PHASE = ("alpha", "rho", "ur", "uth", "uz", "aP_ur", "aP_uth", "aP_uz")
+ASM_DOUBLES_OUT = ("aW", "aE", "aS", "aN", "aB", "aT", "aP", "Su", "pp",
+                   "Fs_r", "Fs_th", "Fs_z", "ac_r", "ac_th", "ac_z", "Fc_r", "Fc_th", "Fc_z")
+ASM_INTS = ("cell_type", "outlet", "act_l", "act_g", "lk_r", "lk_th", "lk_z")
+
+
+class AssemblyFields:
+    """Inputs and outputs of the pressure-equation assembly for one mesh."""
+
+    def __init__(self, nr, nth, nz, flags, scalars):
+        self.nr, self.nth, self.nz = nr, nth, nz
+        self.flags = flags          # 1 liq_room valid, 2 gas in eq., 4 gas compressibility
+        self.scalars = scalars      # dt, rho_gas, T_ambient, beta_expansion
+
+    def copy(self):
+        c = AssemblyFields(self.nr, self.nth, self.nz, self.flags, list(self.scalars))
+        for k, v in self.__dict__.items():
+            if isinstance(v, np.ndarray):
+                setattr(c, k, v.copy())
+        return c
+
+    def doubles(self):
+        out = [getattr(self, n) for n in ASM_DOUBLES_IN]
+        out += [getattr(self, "liq_" + n) for n in ASM_PHASE] + [self.liq_T]
+        out += [getattr(self, "gas_" + n) for n in ASM_PHASE] + [self.gas_T_old]
+        out += [getattr(self, n) for n in ASM_DOUBLES_OUT]
+        return out
+
+    def ints(self):
+        return [getattr(self, n) for n in ASM_INTS]
+
+    def outputs(self):
+        names = list(ASM_DOUBLES_OUT) + ["lk_r", "lk_th", "lk_z"]
+        return {n: getattr(self, n) for n in names}
+
+
+def make_assembly_fields(nr: int, nth: int, nz: int, seed: int = 0, flags: int = 7,
+                         solid_frac: float = 0.05, sealed_frac: float = 0.08,
+                         dt: float = 1e-3) -> AssemblyFields:
+    """Seeded inputs of the pressure-equation assembly: uniform cell centres
+    and metric arrays, a pressure field, liquid (steel: rho ~7000, T ~1800 K)
+    and gas (rho ~0.3, previous T 300-3000 K) states with volume fractions,
+    velocities and momentum diagonals (some at or below SMALL), activity
+    masks leaving some sealed cells, a liquid-room field with some closed
+    pores (<= 1e-4), a few solid cells, electrode holes on the top layer.
+    Output arrays start with random values: the assembly must overwrite them
+    everywhere. Halo entries are random too."""
+    rng = np.random.default_rng(seed)
+    shp = halo_shape(nr, nth, nz)
+    f = AssemblyFields(nr, nth, nz, flags, [dt, RHO_GAS, 300.0, 1.0e-4])
+    f.vol = rng.uniform(0.5, 1.5, size=shp) * 1e-2
+    for n in ("Ar", "Ath", "Az"):
+        setattr(f, n, rng.uniform(0.5, 1.5, size=shp) * 1e-1)
+    f.r = (np.arange(-1, nr + 3) - 0.5) * (R_FURNACE / nr)
+    f.theta = (np.arange(-1, nth + 3) - 0.5) * (2.0 * math.pi / nth)
+    f.z = (np.arange(-1, nz + 3) - 0.5) * (H_FURNACE / nz)
+    f.p = rng.normal(0.0, 1e3, size=shp)
+    f.liq_room = rng.uniform(0.0, 1.0, size=shp)
+    f.liq_room[rng.random(shp) < 0.1] = 5e-5
+    for ph, rho, T in (("liq", 7000.0, 1800.0), ("gas", 0.3, 1500.0)):
+        setattr(f, ph + "_alpha", rng.uniform(0.0, 1.0, size=shp))
+        setattr(f, ph + "_rho", rho * rng.uniform(0.8, 1.2, size=shp))
+        for c in ("ur", "uth", "uz"):
+            setattr(f, ph + "_" + c, rng.normal(0.0, 0.5, size=shp))
+        for c in ("aP_ur", "aP_uth", "aP_uz"):
+            a = rng.uniform(1.0, 1e3, size=shp)
+            a[rng.random(shp) < 0.05] = 1e-31
+            setattr(f, ph + "_" + c, a)
+    f.liq_T = 1800.0 * rng.uniform(0.9, 1.1, size=shp)
+    f.gas_T_old = rng.uniform(50.0, 3000.0, size=shp)
+    f.cell_type = (rng.random(shp) >= solid_frac).astype(np.int32)
+    u = rng.random(shp)
+    f.act_l = (u < 0.6).astype(np.int32)
+    f.act_g = ((u >= 0.35) & (u < 1.0 - sealed_frac)).astype(np.int32)
+    f.outlet = np.zeros(shp, dtype=np.int32)
+    f.outlet[nz + 1][rng.random(shp[1:]) < 0.1] = 1
+    f.outlet[rng.random(shp) < 0.02] = 1   # ignored below the top layer
+    for n in ASM_DOUBLES_OUT:
+        setattr(f, n, rng.normal(size=shp))
+    for n in ("lk_r", "lk_th", "lk_z"):
+        setattr(f, n, rng.integers(0, 3, size=shp).astype(np.int32))
+    return f
+
+
 def system_bytes(nr: int, nth: int, nz: int) -> int:
     """Host bytes of one system (8 halo-layout FP64 arrays)."""
     return 8 * 8 * (nr + 4) * (nth + 4) * (nz + 4)

@@ -212,6 +212,49 @@ int eaf_pressure_correct_f64(eaf_cg_t h, const eaf_pcorr_fields_t* f);
  * before return). */
 int eaf_pressure_correct_f64_device(eaf_cg_t h, const eaf_pcorr_fields_t* f);
 
+/* Assembly of the pressure-correction equation: replaces the serial code of
+ * solve_pressure_correction before the CG (src/mod_pressure_3d.f90:135-310):
+ * cell pressure gradients of each phase (cell_gradients :621-651, the gas
+ * one with the liquid-weight correction), the Rhie-Chow face contributions of
+ * the liquid and, when it is in the equation, of the gas
+ * (add_phase_contribution :469-619), the gas compressibility source, the
+ * diagonal with compliance and acoustic terms, the boundary folding
+ * (apply_pressure_bc, src/mod_boundary_3d.f90:180-277) and the continuity
+ * residual sum|Su| / flux_ref. Outputs: aW..Su and pp (zeroed), the
+ * liquid's exported face terms Fs_*, ac_* and link flags lk_* (Fc_* zeroed),
+ * every array overwritten over the whole halo layout -- bit-identical to the
+ * serial Fortran; the residual's two sums are associated per block (within
+ * 1e-12 of the sequential sums). Activity masks and the liquid room are the
+ * caller's (they come from the phase state). Fortran MAX/MIN on NaN are not
+ * pinned. Layouts as eaf_pcorr_fields_t; `outlet` marks electrode holes on
+ * the top layer (k = nz). Gas fields may be NULL when neither gas switch is
+ * set (gas_T_old, gas alpha and rho are read for compressibility alone). */
+typedef struct {
+  const double *alpha, *rho, *ur, *uth, *uz, *aP_ur, *aP_uth, *aP_uz;
+} eaf_phase_state_t;
+
+typedef struct {
+  const int *cell_type, *outlet, *act_l, *act_g;
+  const double *vol, *Ar, *Ath, *Az;
+  const double *r, *theta, *z;            /* cell centres, index -1..n+2 */
+  const double *p, *liq_room;
+  eaf_phase_state_t liq, gas;
+  const double *liq_T, *gas_T_old;
+  int liq_room_valid;                     /* ws_liq_room_valid */
+  int gas_in_poisson;                     /* gas_in_poisson .and. solve_multiphase */
+  int gas_compressibility;                /* gas_compressibility .and. solve_multiphase */
+  double dt, rho_gas, T_ambient, beta_expansion;
+  double *aW, *aE, *aS, *aN, *aB, *aT, *aP, *Su, *pp;
+  double *Fs_r, *Fs_th, *Fs_z, *ac_r, *ac_th, *ac_z, *Fc_r, *Fc_th, *Fc_z;
+  int *lk_r, *lk_th, *lk_z;
+} eaf_assembly_fields_t;
+
+/* Host arrays (uploaded to the handle's mirror, outputs downloaded). */
+int eaf_pressure_assemble_f64(eaf_cg_t h, const eaf_assembly_fields_t* f, double* residual);
+/* Device arrays, assembled in place on the handle's stream. */
+int eaf_pressure_assemble_f64_device(eaf_cg_t h, const eaf_assembly_fields_t* f,
+                                     double* residual);
+
 /* Multi-rank drop-in helpers (host-side index work, no device and no MPI):
  * an MPI-decomposed run (m%is_parallel) gathers its blocks onto one rank,
  * solves there on the GPU and scatters the solution back.

@@ -55,6 +55,10 @@ def lib():
                                                   ctypes.POINTER(ctypes.POINTER(ci)),
                                                   ci, cd]
         L.eaf_oracle_pressure_correct.restype = ci
+        L.eaf_oracle_pressure_assemble.argtypes = [ci, ci, ci, ctypes.POINTER(_dp),
+                                                   ctypes.POINTER(ctypes.POINTER(ci)),
+                                                   ci, _dp, _dp]
+        L.eaf_oracle_pressure_assemble.restype = ci
         L.eaf_oracle_max_threads.argtypes = []
         L.eaf_oracle_max_threads.restype = ci
         _lib = L
@@ -140,6 +144,27 @@ def pressure_correct(f) -> None:
                                            1 if f.has_gas else 0, float(f.alpha_p))
     if rc != 0:
         raise RuntimeError(f"oracle pressure_correct failed with status {rc}")
+
+
+def pressure_assemble(f) -> float:
+    """Serial assembly of the pressure-correction equation
+    (src/mod_pressure_3d.f90:135-310) in place on the output arrays of an
+    eafgen.AssemblyFields; returns the continuity residual."""
+    ci = ctypes.c_int
+    dv, iv = f.doubles(), f.ints()
+    for a in dv:
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    for a in iv:
+        assert a.dtype == np.int32 and a.flags.c_contiguous
+    darr = (_dp * len(dv))(*[a.ctypes.data_as(_dp) for a in dv])
+    iarr = (ctypes.POINTER(ci) * len(iv))(*[a.ctypes.data_as(ctypes.POINTER(ci)) for a in iv])
+    sc = (ctypes.c_double * 4)(*f.scalars)
+    res = ctypes.c_double()
+    rc = lib().eaf_oracle_pressure_assemble(f.nr, f.nth, f.nz, darr, iarr, int(f.flags), sc,
+                                            ctypes.byref(res))
+    if rc != 0:
+        raise RuntimeError(f"oracle pressure_assemble failed with status {rc}")
+    return res.value
 
 
 def max_threads() -> int:

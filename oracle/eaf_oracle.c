@@ -41,7 +41,13 @@
  *   - flux export, halo refresh, velocity and pressure corrections, sealed
  *     cells ..................................... src/mod_pressure_3d.f90:333-397
  *   - correct_velocities ........................ src/mod_pressure_3d.f90:689-746
- * (eaf_oracle_pressure_correct).
+ * (eaf_oracle_pressure_correct), and the assembly before the CG
+ *   - masks in, gradients, phase contributions, compressibility, aP,
+ *     boundary folding, continuity residual .... src/mod_pressure_3d.f90:135-310
+ *     (cell_gradients :621-651, add_phase_contribution :469-619, helpers
+ *     :405-458, :654-681; pgrad src/mod_constants.f90:274-287;
+ *     apply_pressure_bc src/mod_boundary_3d.f90:180-277)
+ * (eaf_oracle_pressure_assemble).
  *
  * PARITY UNPINNED: the reference is Fortran + MPI and no Fortran compiler or
  * MPI exists where this is built or run, and the reference's tests pin only
@@ -725,5 +731,339 @@ int eaf_oracle_pressure_correct(int nr, int nth, int nz, double* const* dv, int*
             }
     /* 6. (:396) */
     eaf_oracle_theta_wrap(nr, nth, nz, p);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Assembly of the pressure-correction equation, serial branch of
+ * solve_pressure_correction up to the CG call (src/mod_pressure_3d.f90:
+ * 135-310), in the reference's statement and operand order.
+ * dv (double, halo layout unless noted):
+ *   0 vol, 1 Ar, 2 Ath, 3 Az, 4 r, 5 theta, 6 z (cell centres, -1..n+2),
+ *   7 p, 8 liq_room,
+ *   9-16 liquid alpha, rho, ur, uth, uz, aP_ur, aP_uth, aP_uz, 17 liquid T,
+ *   18-25 gas (same order), 26 gas T_old,
+ *   outputs 27-35 aW, aE, aS, aN, aB, aT, aP, Su, pp,
+ *           36-44 Fs_r, Fs_th, Fs_z, ac_r, ac_th, ac_z, Fc_r, Fc_th, Fc_z.
+ * iv (int, halo layout): 0 cell_type, 1 outlet (nonzero: electrode hole at
+ *   k = nz), 2 act_l, 3 act_g, outputs 4-6 lk_r, lk_th, lk_z.
+ * flags: 1 liq_room_valid, 2 gas in the pressure equation, 4 gas
+ *   compressibility. sc: dt, rho_gas, T_ambient, beta_expansion.
+ * Fortran MAX/MIN are fmax/fmin (identical on non-NaN values).
+ * ---------------------------------------------------------------------- */
+#define GRAVITY_C 9.81
+#define PP_COMPLIANCE_C 1.0e-6
+#define COMP_SRC_CAP_C 0.2
+#define P0_THERMO_C 101325.0
+#define C_SOUND_LIQ_C 4000.0
+#define T_MIN_GAS_C 100.0
+#define ROOM_EPS_C 1.0e-4
+
+typedef struct {
+    const dims_t* d;
+    double* const* dv;
+    int* const* iv;
+    int flags;
+    const double* sc;
+} asm_t;
+
+static inline int pv_cell(const asm_t* A, size_t q) {
+    return A->iv[0][q] != 0 && (A->iv[2][q] || A->iv[3][q]);
+}
+
+/* pgrad (src/mod_constants.f90:274-287) */
+static double pgrad(double pm, double p0, double pp_, double xm, double x0, double xp,
+                    int okm, int okp) {
+    if (okm && okp) return (pp_ - pm) / (xp - xm);
+    if (okp) return (pp_ - p0) / (xp - x0);
+    if (okm) return (p0 - pm) / (x0 - xm);
+    return 0.0;
+}
+
+/* liq_weight_f (:407-417) between cells qa and qb of one column */
+static double liq_weight_f(const asm_t* A, size_t qa, size_t qb) {
+    const double *al = A->dv[9], *rho = A->dv[10], *T = A->dv[17];
+    const int* act = A->iv[2];
+    const double beta = A->sc[3], Tamb = A->sc[2];
+    return 0.5 * GRAVITY_C *
+           ((act[qa] ? 1.0 : 0.0) * al[qa] * rho[qa] * (1.0 - beta * (T[qa] - Tamb)) +
+            (act[qb] ? 1.0 : 0.0) * al[qb] * rho[qb] * (1.0 - beta * (T[qb] - Tamb)));
+}
+
+/* cell_gradients (:621-651) of p into gr, gth, gz (whole arrays zeroed,
+ * interior non-solid cells computed, theta halos refreshed); with isg the
+ * vertical gradient is gas_gz (:421-440). */
+static void cell_gradients(const asm_t* A, int isg, double* gr, double* gth, double* gz) {
+    const dims_t* d = A->d;
+    const double *p = A->dv[7], *r = A->dv[4], *th = A->dv[5], *z = A->dv[6];
+    memset(gr, 0, d->n * sizeof(double));
+    memset(gth, 0, d->n * sizeof(double));
+    memset(gz, 0, d->n * sizeof(double));
+    for (int k = 1; k <= d->nz; ++k)
+        for (int j = 1; j <= d->nth; ++j)
+            for (int i = 1; i <= d->nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (A->iv[0][q] == 0) continue;
+                const size_t qw = q - 1, qe = q + 1, qs = q - d->sx, qn = q + d->sx,
+                             qb = q - d->sxy, qt = q + d->sxy;
+                gr[q] = pgrad(p[qw], p[q], p[qe], r[i], r[i + 1], r[i + 2],
+                              i > 1 && pv_cell(A, qw), i < d->nr && pv_cell(A, qe));
+                gth[q] = pgrad(p[qs], p[q], p[qn], r[i + 1] * th[j], r[i + 1] * th[j + 1],
+                               r[i + 1] * th[j + 2], pv_cell(A, qs), pv_cell(A, qn));
+                const int okm = k > 1 && pv_cell(A, qb), okp = k < d->nz && pv_cell(A, qt);
+                gz[q] = pgrad(p[qb], p[q], p[qt], z[k], z[k + 1], z[k + 2], okm, okp);
+                if (isg) {
+                    double gb = 0.0, gt = 0.0, g;
+                    if (okm) gb = (p[q] - p[qb]) / (z[k + 1] - z[k]) + liq_weight_f(A, qb, q);
+                    if (okp) gt = (p[qt] - p[q]) / (z[k + 2] - z[k + 1]) + liq_weight_f(A, q, qt);
+                    if (okm && okp) g = 0.5 * (gb + gt);
+                    else if (okp) g = gt;
+                    else if (okm) g = gb;
+                    else g = 0.0;
+                    gz[q] = g;
+                }
+            }
+    eaf_oracle_theta_wrap(d->nr, d->nth, d->nz, gr);
+    eaf_oracle_theta_wrap(d->nr, d->nth, d->nz, gth);
+    eaf_oracle_theta_wrap(d->nr, d->nth, d->nz, gz);
+}
+
+/* face_open (:660-668) */
+static int face_open(const asm_t* A, int isg, double u_f, double room_neg, double room_pos) {
+    if (isg || !(A->flags & 1)) return 1;
+    int open = 1;
+    if (u_f > 0.0 && room_pos <= ROOM_EPS_C) open = 0;
+    if (u_f < 0.0 && room_neg <= ROOM_EPS_C) open = 0;
+    return open;
+}
+
+/* add_phase_contribution (:469-619) of one phase (ph = dv index of its
+ * alpha; aef = its alpha), accumulating into the coefficients, Su and
+ * flux_ref; export writes the + faces' Fs/ac/lk. */
+static void add_phase(const asm_t* A, int ph, const int* act, int export_, const double* gr,
+                      const double* gth, const double* gz, int isg, double* flux_ref) {
+    const dims_t* d = A->d;
+    double* const* dv = A->dv;
+    const double *aef = dv[ph], *ur = dv[ph + 2], *uth = dv[ph + 3], *uz = dv[ph + 4],
+                 *apr = dv[ph + 5], *apt = dv[ph + 6], *apz = dv[ph + 7];
+    const double *vol = dv[0], *Ar = dv[1], *Ath = dv[2], *Az = dv[3], *r = dv[4],
+                 *th = dv[5], *z = dv[6], *pf = dv[7], *rm = dv[8];
+    double *aW = dv[27], *aE = dv[28], *aS = dv[29], *aN = dv[30], *aB = dv[31],
+           *aT = dv[32], *Su = dv[34];
+    double *Fs_r = dv[36], *Fs_th = dv[37], *Fs_z = dv[38], *ac_r = dv[39], *ac_th = dv[40],
+           *ac_z = dv[41];
+    int *lk_r = A->iv[4], *lk_th = A->iv[5], *lk_z = A->iv[6];
+    const int* ct = A->iv[0];
+#define LINK(x) (ct[x] != 0 && act[x])
+#define DF(ap, x) (0.5 * (aef[q] * vol[q] / fmax(ap[q], SMALL) + aef[x] * vol[x] / fmax(ap[x], SMALL)))
+    for (int k = 1; k <= d->nz; ++k)
+        for (int j = 1; j <= d->nth; ++j)
+            for (int i = 1; i <= d->nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (ct[q] == 0) continue;
+                if (!act[q]) continue;
+                const size_t w = q - 1, e = q + 1, s = q - d->sx, n = q + d->sx, b = q - d->sxy,
+                             t = q + d->sxy;
+                double d_f, af, u_f, delta;
+                if (LINK(w)) {
+                    d_f = DF(apr, w);
+                    af = 0.5 * (aef[q] + aef[w]);
+                    delta = r[i + 1] - r[i];
+                    u_f = 0.5 * (ur[w] + ur[q]) +
+                          d_f * (0.5 * (gr[w] + gr[q]) - (pf[q] - pf[w]) / delta);
+                    if (face_open(A, isg, u_f, rm[w], rm[q])) {
+                        aW[q] = aW[q] + af * d_f * Ar[w] / delta;
+                        Su[q] = Su[q] + af * u_f * Ar[w];
+                        *flux_ref = *flux_ref + fabs(af * u_f * Ar[w]);
+                    }
+                }
+                if (LINK(e)) {
+                    d_f = DF(apr, e);
+                    af = 0.5 * (aef[q] + aef[e]);
+                    delta = r[i + 2] - r[i + 1];
+                    u_f = 0.5 * (ur[q] + ur[e]) +
+                          d_f * (0.5 * (gr[q] + gr[e]) - (pf[e] - pf[q]) / delta);
+                    if (face_open(A, isg, u_f, rm[q], rm[e])) {
+                        aE[q] = aE[q] + af * d_f * Ar[q] / delta;
+                        Su[q] = Su[q] - af * u_f * Ar[q];
+                        *flux_ref = *flux_ref + fabs(af * u_f * Ar[q]);
+                        if (export_) {
+                            Fs_r[q] = af * u_f * Ar[q];
+                            ac_r[q] = af * d_f * Ar[q] / delta;
+                            lk_r[q] = 1;
+                        }
+                    }
+                }
+                if (LINK(s)) {
+                    d_f = DF(apt, s);
+                    af = 0.5 * (aef[q] + aef[s]);
+                    delta = r[i + 1] * (th[j + 1] - th[j]);
+                    u_f = 0.5 * (uth[s] + uth[q]) +
+                          d_f * (0.5 * (gth[s] + gth[q]) - (pf[q] - pf[s]) / delta);
+                    if (face_open(A, isg, u_f, rm[s], rm[q])) {
+                        aS[q] = aS[q] + af * d_f * Ath[q] / delta;
+                        Su[q] = Su[q] + af * u_f * Ath[q];
+                        *flux_ref = *flux_ref + fabs(af * u_f * Ath[q]);
+                    }
+                }
+                if (LINK(n)) {
+                    d_f = DF(apt, n);
+                    af = 0.5 * (aef[q] + aef[n]);
+                    delta = r[i + 1] * (th[j + 2] - th[j + 1]);
+                    u_f = 0.5 * (uth[q] + uth[n]) +
+                          d_f * (0.5 * (gth[q] + gth[n]) - (pf[n] - pf[q]) / delta);
+                    if (face_open(A, isg, u_f, rm[q], rm[n])) {
+                        aN[q] = aN[q] + af * d_f * Ath[q] / delta;
+                        Su[q] = Su[q] - af * u_f * Ath[q];
+                        *flux_ref = *flux_ref + fabs(af * u_f * Ath[q]);
+                        if (export_) {
+                            Fs_th[q] = af * u_f * Ath[q];
+                            ac_th[q] = af * d_f * Ath[q] / delta;
+                            lk_th[q] = 1;
+                        }
+                    }
+                }
+                if (LINK(b)) {
+                    d_f = DF(apz, b);
+                    af = 0.5 * (aef[q] + aef[b]);
+                    delta = z[k + 1] - z[k];
+                    const double lw = isg ? liq_weight_f(A, b, q) : 0.0;
+                    u_f = 0.5 * (uz[b] + uz[q]) +
+                          d_f * (0.5 * (gz[b] + gz[q]) - (pf[q] - pf[b]) / delta - lw);
+                    if (face_open(A, isg, u_f, rm[b], rm[q])) {
+                        aB[q] = aB[q] + af * d_f * Az[b] / delta;
+                        Su[q] = Su[q] + af * u_f * Az[b];
+                        *flux_ref = *flux_ref + fabs(af * u_f * Az[b]);
+                    }
+                }
+                if (LINK(t)) {
+                    d_f = DF(apz, t);
+                    af = 0.5 * (aef[q] + aef[t]);
+                    delta = z[k + 2] - z[k + 1];
+                    const double lw = isg ? liq_weight_f(A, q, t) : 0.0;
+                    u_f = 0.5 * (uz[q] + uz[t]) +
+                          d_f * (0.5 * (gz[q] + gz[t]) - (pf[t] - pf[q]) / delta - lw);
+                    if (face_open(A, isg, u_f, rm[q], rm[t])) {
+                        aT[q] = aT[q] + af * d_f * Az[q] / delta;
+                        Su[q] = Su[q] - af * u_f * Az[q];
+                        *flux_ref = *flux_ref + fabs(af * u_f * Az[q]);
+                        if (export_) {
+                            Fs_z[q] = af * u_f * Az[q];
+                            ac_z[q] = af * d_f * Az[q] / delta;
+                            lk_z[q] = 1;
+                        }
+                    }
+                }
+            }
+#undef LINK
+#undef DF
+}
+
+int eaf_oracle_pressure_assemble(int nr, int nth, int nz, double* const* dv, int* const* iv,
+                                 int flags, const double* sc, double* residual) {
+    if (nr < 1 || nth < 1 || nz < 1) return 2;
+    const dims_t D = mkdims(nr, nth, nz);
+    const dims_t* d = &D;
+    asm_t A = {d, dv, iv, flags, sc};
+    const int gas_in = (flags & 2) != 0, gas_comp = (flags & 4) != 0;
+    double* g = (double*)malloc(sizeof(double) * 6 * d->n);
+    if (!g) return 6;
+    double *gpr = g, *gpth = g + d->n, *gpz = g + 2 * d->n;
+    double *gpr_g = g + 3 * d->n, *gpth_g = g + 4 * d->n, *gpz_g = g + 5 * d->n;
+    /* (:140-146, :171-173) whole arrays zeroed */
+    for (int a = 27; a <= 44; ++a) memset(dv[a], 0, d->n * sizeof(double));
+    for (int a = 4; a <= 6; ++a) memset(iv[a], 0, d->n * sizeof(int));
+    /* (:180-185) */
+    cell_gradients(&A, 0, gpr, gpth, gpz);
+    if (gas_in) cell_gradients(&A, 1, gpr_g, gpth_g, gpz_g);
+    /* (:205-210) */
+    double flux_ref = 0.0;
+    add_phase(&A, 9, iv[2], 1, gpr, gpth, gpz, 0, &flux_ref);
+    if (gas_in) add_phase(&A, 18, iv[3], 0, gpr_g, gpth_g, gpz_g, 1, &flux_ref);
+    double *aW = dv[27], *aE = dv[28], *aS = dv[29], *aN = dv[30], *aB = dv[31],
+           *aT = dv[32], *aP = dv[33], *Su = dv[34];
+    const int *ct = iv[0], *out = iv[1], *act_l = iv[2], *act_g = iv[3];
+    const double *vol = dv[0], *al_g = dv[18], *rho_g = dv[19], *Told = dv[26],
+                 *al_l = dv[9], *rho_l = dv[10];
+    const double dt = sc[0], rho_gas = sc[1], Tamb = sc[2];
+    /* (:228-247) gas compressibility source */
+    if (gas_comp) {
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= nth; ++j)
+                for (int i = 1; i <= nr; ++i) {
+                    const size_t q = at(d, i, j, k);
+                    if (ct[q] == 0) continue;
+                    if (!act_g[q]) continue;
+                    const double src = al_g[q] * vol[q] / dt *
+                                       (rho_g[q] - rho_gas * Tamb / fmax(Told[q], T_MIN_GAS_C)) /
+                                       fmax(rho_g[q], SMALL);
+                    const double cap = COMP_SRC_CAP_C * al_g[q] * vol[q] / dt;
+                    Su[q] = Su[q] - fmax(-cap, fmin(cap, src));
+                }
+    }
+    /* (:250-285) trivial cells and the diagonal */
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= nth; ++j)
+            for (int i = 1; i <= nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (ct[q] == 0) continue;
+                if (!act_l[q] && !act_g[q]) {
+                    aW[q] = 0.0; aE[q] = 0.0; aS[q] = 0.0; aN[q] = 0.0;
+                    aB[q] = 0.0; aT[q] = 0.0; aP[q] = 1.0; Su[q] = 0.0;
+                } else {
+                    aP[q] = (aW[q] + aE[q] + aS[q] + aN[q] + aB[q] + aT[q]) *
+                            (1.0 + PP_COMPLIANCE_C);
+                    if (gas_comp && act_g[q])
+                        aP[q] = aP[q] + al_g[q] / P0_THERMO_C * vol[q] / dt;
+                    if (act_l[q])
+                        aP[q] = aP[q] + al_l[q] * vol[q] /
+                                            (rho_l[q] * (C_SOUND_LIQ_C * C_SOUND_LIQ_C) * dt);
+                }
+            }
+    /* apply_pressure_bc (src/mod_boundary_3d.f90:180-277), serial */
+#define OUT(x) (out[x] != 0 && (x) / d->sxy == (size_t)(nz + 1))
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= nth; ++j)
+            for (int i = 1; i <= nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (ct[q] == 0) {
+                    aW[q] = 0.0; aE[q] = 0.0; aS[q] = 0.0; aN[q] = 0.0;
+                    aB[q] = 0.0; aT[q] = 0.0; aP[q] = 1.0; Su[q] = 0.0;
+                    continue;
+                }
+                if (i == 1) aW[q] = 0.0;
+                if (i == nr) aE[q] = 0.0;
+                if (k == 1) aB[q] = 0.0;
+                if (k == nz) {
+                    if (OUT(q)) {
+                        aW[q] = 0.0; aE[q] = 0.0; aS[q] = 0.0; aN[q] = 0.0;
+                        aB[q] = 0.0; aT[q] = 0.0; aP[q] = 1.0; Su[q] = 0.0;
+                        continue;
+                    }
+                    aT[q] = 0.0;
+                }
+                if (i > 1 && ct[q - 1] == 0) aW[q] = 0.0;
+                if (i < nr && ct[q + 1] == 0) aE[q] = 0.0;
+                if (k > 1 && ct[q - d->sxy] == 0) aB[q] = 0.0;
+                if (k < nz && ct[q + d->sxy] == 0) aT[q] = 0.0;
+                if (OUT(q - 1)) aW[q] = 0.0;
+                if (OUT(q + 1)) aE[q] = 0.0;
+                if (OUT(q - d->sx)) aS[q] = 0.0;
+                if (OUT(q + d->sx)) aN[q] = 0.0;
+                if (OUT(q - d->sxy)) aB[q] = 0.0;
+                if (OUT(q + d->sxy)) aT[q] = 0.0;
+            }
+#undef OUT
+    /* (:292-307) continuity residual */
+    double sum_su = 0.0;
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= nth; ++j)
+            for (int i = 1; i <= nr; ++i) {
+                const size_t q = at(d, i, j, k);
+                if (ct[q] == 0) continue;
+                if (act_l[q] || act_g[q]) sum_su = sum_su + fabs(Su[q]);
+            }
+    *residual = sum_su / fmax(flux_ref, SMALL);
+    free(g);
     return 0;
 }

@@ -56,3 +56,36 @@ def test_invalid_arguments_without_gpu():
         eaf._lib.EAF_EUNSUPPORTED
     assert lib.eaf_cg_destroy(None) == eaf._lib.EAF_EINVAL
     assert lib.eaf_selftest_barrier_timeout(0, -1.0) == eaf._lib.EAF_EINVAL
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """ctypes mirrors of the public structs have the C compiler's sizes and
+    field offsets."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    from importlib import import_module
+    L = import_module("hornofusion-full3d_b200._lib")
+    structs = {"eaf_pcorr_fields_t": L.PcorrFieldsC,
+               "eaf_assembly_fields_t": L.AssemblyFieldsC,
+               "eaf_phase_state_t": L.PhaseState,
+               "eaf_phase_fields_t": L.PhaseFields}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "eafcg.h"',
+             "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0; }"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(exe)], check=True)
+    got = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in got.splitlines():
+        cname, field, val = line.split()
+        py = structs[cname]
+        want = ctypes.sizeof(py) if field == "size" else getattr(py, field).offset
+        assert int(val) == want, (cname, field)
