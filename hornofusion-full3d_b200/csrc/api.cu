@@ -589,7 +589,7 @@ int run_assemble(eaf_cg* h, const eaf_assembly_fields_t& f) {
   EAF_CUDA(cudaMemcpyAsync(&h->res_h->residual,
                            eaf::assembly_result(h->asm_s, h->nr, h->nth, h->nz),
                            sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  h->last_kernels = 3;
+  h->last_kernels = 4;
   return EAF_OK;
 }
 

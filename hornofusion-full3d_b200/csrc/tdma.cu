@@ -35,6 +35,7 @@
 
 #include "cg_common.cuh"
 #include "cg_kernels.h"
+#include "recipdiv.cuh"
 #include "stencil.cuh"
 #include "eafcg.h"
 
@@ -118,35 +119,10 @@ __device__ void theta_wrap(const TdmaArgs& a) {
 
 constexpr int kTdmaMaxLine = 1024;  // 32 elements per lane in a hand-over mask
 
-// ---------------------------------------------------------------------------
-// Correctly rounded t / m from a precomputed y = RN(1/m), by one correction
-// step (Markstein, "Computation of elementary functions on the IBM RISC
-// System/6000 processor", IBM J. Res. Dev. 34(1), 1990, Theorem 1): with
-// q = RN(t*y) within one ulp of t/m, the residual r = t - m*q is exact in an
-// FMA and RN(q + r*y) is the correctly rounded quotient -- the value `/`
-// returns. The theorem needs the operands away from overflow and underflow:
-// both exponents in [-500, 500] (then q, r and r*y are normal); anything else
-// -- zeros, subnormals, huge values, infinities, NaN -- takes `/` itself. The
-// point is latency: the reciprocal leaves the sweep's dependent chain.
-// ---------------------------------------------------------------------------
 // Empty hand-over slot: a signalling NaN (IEEE arithmetic only delivers
 // quiet NaNs, so no solution value has this pattern).
 #define kEmptySlot __longlong_as_double(0x7ff000017ff00001ll)
 constexpr unsigned long long kEmptyBits = 0x7ff000017ff00001ull;
-
-__device__ __forceinline__ bool exp_in_safe_range(double v) {
-  const unsigned e = (unsigned)((unsigned long long)__double_as_longlong(v) >> 52) & 0x7ffu;
-  return e - 523u <= 1000u;  // biased exponent 523..1523
-}
-
-__device__ __forceinline__ double div_by_recip(double t, double m, double y, bool m_ok) {
-  if (m_ok && (t == 0.0 || exp_in_safe_range(t))) {
-    const double q = t * y;
-    const double c = __fma_rn(__fma_rn(-q, m, t), y, q);
-    return t == 0.0 ? q : c;
-  }
-  return t / m;
-}
 
 // Line factors: the phi-independent half of `tdma` (src/mod_solver_3d.f90:
 // 30-38) -- the guarded pivots m_i = b_i - a_i cp_{i-1} (b_1 for i = 1) and

@@ -24,7 +24,10 @@
 ! and the post-CG corrections of solve_pressure_correction
 ! (src/mod_pressure_3d.f90:333-397 with correct_velocities :689-746) become
 ! one call of pressure_correct_gpu (fill an eaf_pcorr_fields with c_loc of
-! the arrays; see its comment).
+! the arrays; see its comment), and the assembly of the pressure-correction
+! equation before the CG (src/mod_pressure_3d.f90:135-310 with
+! apply_pressure_bc, src/mod_boundary_3d.f90:180-277) one call of
+! pressure_assemble_gpu (an eaf_assembly_fields).
 !===============================================================================
 module mod_solver_gpu
     use iso_c_binding
@@ -35,6 +38,7 @@ module mod_solver_gpu
     public :: eaf_cg_create, eaf_cg_destroy, eaf_cg_solve_f64, eaf_cg_solve_mixed
     public :: eaf_tdma_3d_f64, eaf_residual_3d_f64
     public :: eaf_phase_fields, eaf_pcorr_fields, pressure_correct_gpu
+    public :: eaf_phase_state, eaf_assembly_fields, pressure_assemble_gpu
     public :: cg_3d_gpu_mpi
 
     integer(c_int), parameter, public :: EAF_OK = 0, EAF_ENONFINITE = 3
@@ -54,6 +58,27 @@ module mod_solver_gpu
         integer(c_int) :: has_gas
         real(c_double) :: alpha_p
     end type eaf_pcorr_fields
+
+    ! Mirrors of eaf_phase_state_t / eaf_assembly_fields_t: the inputs of
+    ! the assembly (c_loc of the mesh, state and mask arrays; outlet is the
+    ! out_mask of apply_pressure_bc, nonzero where an electrode hole covers a
+    ! top-layer cell; act_l / act_g and liq_room as the caller computes them
+    ! for the phase loops), the switches and scalars, and the outputs.
+    type, bind(C) :: eaf_phase_state
+        type(c_ptr) :: alpha, rho, ur, uth, uz, aP_ur, aP_uth, aP_uz
+    end type eaf_phase_state
+
+    type, bind(C) :: eaf_assembly_fields
+        type(c_ptr) :: cell_type, outlet, act_l, act_g
+        type(c_ptr) :: vol, Ar, Ath, Az, r, theta, z, p, liq_room
+        type(eaf_phase_state) :: liq, gas
+        type(c_ptr) :: liq_T, gas_T_old
+        integer(c_int) :: liq_room_valid, gas_in_poisson, gas_compressibility
+        real(c_double) :: dt, rho_gas, T_ambient, beta_expansion
+        type(c_ptr) :: aW, aE, aS, aN, aB, aT, aP, Su, pp
+        type(c_ptr) :: Fs_r, Fs_th, Fs_z, ac_r, ac_th, ac_z, Fc_r, Fc_th, Fc_z
+        type(c_ptr) :: lk_r, lk_th, lk_z
+    end type eaf_assembly_fields
 
     interface
         integer(c_int) function eaf_cg_create(h, nr, nth, nz, device) &
@@ -178,6 +203,14 @@ module mod_solver_gpu
             type(c_ptr), value :: h
             type(eaf_pcorr_fields), intent(in) :: f
         end function eaf_pressure_correct_f64
+
+        integer(c_int) function eaf_pressure_assemble_f64(h, f, residual) &
+                bind(C, name="eaf_pressure_assemble_f64")
+            import :: c_int, c_ptr, c_double, eaf_assembly_fields
+            type(c_ptr), value :: h
+            type(eaf_assembly_fields), intent(in) :: f
+            real(c_double), intent(out) :: residual
+        end function eaf_pressure_assemble_f64
     end interface
 
     ! One handle per mesh size, kept across SIMPLE iterations like the
@@ -309,6 +342,30 @@ contains
         st = eaf_pressure_correct_f64(handle, f)
         if (st /= EAF_OK) error stop 'eaf_pressure_correct_f64 failed'
     end subroutine pressure_correct_gpu
+
+    ! Replaces src/mod_pressure_3d.f90:135-310 up to the CG (coefficient
+    ! arrays and pp zeroed, cell gradients of both phases, the liquid's and
+    ! the gas's face contributions with the exported Fs_*, ac_* and link
+    ! flags, the gas compressibility source, trivial rows and the diagonal,
+    ! apply_pressure_bc, the continuity residual sum|Su| / flux_ref): the
+    ! caller fills f with c_loc of the workspace and state arrays, the
+    ! switches (ws_liq_room_valid, cfg%gas_in_poisson .and.
+    ! cfg%solve_multiphase, cfg%gas_compressibility .and.
+    ! cfg%solve_multiphase) and scalars (dt, RHO_GAS, T_AMBIENT,
+    ! BETA_EXPANSION). Every array is bit-identical to the serial Fortran;
+    ! the residual agrees to 1e-12 relative (its sums are associated per
+    ! block). Serial meshes only.
+    subroutine pressure_assemble_gpu(f, m, residual)
+        use mod_types_3d, only: mesh_t
+        type(eaf_assembly_fields), intent(in) :: f
+        type(mesh_t), intent(in) :: m
+        real(c_double), intent(out) :: residual
+        integer(c_int) :: st
+        if (m%is_parallel) error stop 'pressure_assemble_gpu: decomposed meshes are not supported'
+        call ensure_handle(m%nr, m%ntheta, m%nz)
+        st = eaf_pressure_assemble_f64(handle, f, residual)
+        if (st /= EAF_OK) error stop 'eaf_pressure_assemble_f64 failed'
+    end subroutine pressure_assemble_gpu
 
     ! Same dummies as cg_3d_mpi for DECOMPOSED meshes (m%is_parallel): the
     ! blocks of the eight coefficient arrays and phi are gathered onto rank 0

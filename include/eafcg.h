@@ -227,8 +227,12 @@ int eaf_pressure_correct_f64_device(eaf_cg_t h, const eaf_pcorr_fields_t* f);
  * 1e-12 of the sequential sums). Activity masks and the liquid room are the
  * caller's (they come from the phase state). Fortran MAX/MIN on NaN are not
  * pinned. Layouts as eaf_pcorr_fields_t; `outlet` marks electrode holes on
- * the top layer (k = nz). Gas fields may be NULL when neither gas switch is
- * set (gas_T_old, gas alpha and rho are read for compressibility alone). */
+ * the top layer (k = nz; out_mask of apply_pressure_bc). Arrays the switches
+ * leave unread may be NULL: liq_room without liq_room_valid, liq_T and the
+ * gas velocities and momentum diagonals without gas_in_poisson, gas alpha
+ * and rho without either gas switch, gas_T_old without gas_compressibility.
+ * Output arrays must not overlap input arrays. dt must be > 0; meshes up to
+ * 2^31 halo elements (else EAF_EUNSUPPORTED). */
 typedef struct {
   const double *alpha, *rho, *ur, *uth, *uz, *aP_ur, *aP_uth, *aP_uz;
 } eaf_phase_state_t;

@@ -64,7 +64,7 @@ def check(f):
 @pytest.mark.parametrize("flags", [0, 1, 3, 6, 7])
 def test_assembly_bitwise_small(dims, flags):
     t = check(gen().make_assembly_fields(*dims, seed=11, flags=flags))
-    assert t["kernels"] == 3
+    assert t["kernels"] == 4
 
 
 def test_assembly_all_solid_and_all_sealed():
