@@ -109,7 +109,7 @@ __device__ __forceinline__ void cell_of(const AsmArgs& a, unsigned q, int& i, in
 // one: the stencil's masks and pressures, the coordinates, and (gas) the
 // liquid columns for the weights.
 template <bool GAS_IN>
-__global__ void __launch_bounds__(kAsmBlock) asm_gradient_kernel(AsmArgs a) {
+__global__ void __launch_bounds__(kAsmBlock, 4) asm_gradient_kernel(AsmArgs a) {
   const eaf_assembly_fields_t& f = a.f;
   for (unsigned qd = blockIdx.x * blockDim.x + threadIdx.x; qd < a.nh;
        qd += gridDim.x * blockDim.x) {
@@ -479,15 +479,17 @@ __global__ void __launch_bounds__(kAsmBlock, 2) asm_cell_kernel(AsmArgs a) {
   }
 }
 
-// One warp: lane l sums block partials l, l+32, ... in order, then the
-// butterfly; residual = sum_su / max(flux_ref, SMALL) (:305).
-__global__ void asm_residual_kernel(AsmArgs a, int nblocks) {
-  double s[2];
-  for (int m = 0; m < 2; ++m) {
-    double acc = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += 32) acc = acc + a.part[m * nblocks + b];
-    s[m] = warp_allsum(acc);
+// One block: thread t sums block partials t, t + blockDim, ... in order, then
+// a fixed-order block reduction; residual = sum_su / max(flux_ref, SMALL)
+// (:305). Deterministic for a given grid.
+constexpr int kAsmResBlock = 1024;
+__global__ void __launch_bounds__(kAsmResBlock) asm_residual_kernel(AsmArgs a, int nblocks) {
+  double s[2] = {0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    s[0] = s[0] + a.part[b];
+    s[1] = s[1] + a.part[nblocks + b];
   }
+  block_sum_to_thread0<2, double>(s);
   if (threadIdx.x == 0) *a.result = s[1] / fmax(s[0], kS);
 }
 
@@ -553,7 +555,7 @@ cudaError_t launch_assemble_f64(const eaf_assembly_fields_t& f, int nr, int nth,
   cells[(gi ? 2 : 0) + (gc ? 1 : 0)]<<<gf, kAsmBlock, 0, st>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  asm_residual_kernel<<<1, 32, 0, st>>>(a, (int)gf);
+  asm_residual_kernel<<<1, kAsmResBlock, 0, st>>>(a, (int)gf);
   return cudaGetLastError();
 }
 
