@@ -163,15 +163,9 @@ class CGSolver:
               else self._lib.eaf_pressure_correct_f64)
         check(fn(self._h, ctypes.byref(c)), "eaf_pressure_correct_f64")
 
-    def pressure_assemble(self, fields, device_ptrs: bool = False) -> float:
-        """Assembly of the pressure-correction equation (solve_pressure_correction
-        up to the CG, src/mod_pressure_3d.f90:135-310, with apply_pressure_bc,
-        src/mod_boundary_3d.f90:180-277) into the output arrays of ``fields``
-        (an object with the attributes of eafgen.AssemblyFields: float64
-        halo-layout arrays, int32 masks, coordinate arrays, ``flags`` -- 1
-        liquid room valid, 2 gas in the equation, 4 gas compressibility -- and
-        ``scalars`` = (dt, rho_gas, T_ambient, beta_expansion)). Returns the
-        continuity residual sum|Su| / flux_ref."""
+    def _assembly_struct(self, fields):
+        """eaf_assembly_fields_t of ``fields`` (numpy arrays or device
+        tensors; attributes the switches leave unread may be None)."""
         from ._lib import ASSEMBLY_IN, ASSEMBLY_OUT, AssemblyFieldsC, PhaseState
 
         ints = ("cell_type", "outlet", "act_l", "act_g", "lk_r", "lk_th", "lk_z")
@@ -201,11 +195,41 @@ class CGSolver:
         c.liq_room_valid, c.gas_in_poisson, c.gas_compressibility = \
             fl & 1, (fl >> 1) & 1, (fl >> 2) & 1
         c.dt, c.rho_gas, c.T_ambient, c.beta_expansion = [float(x) for x in fields.scalars]
+        return c
+
+    def pressure_assemble(self, fields, device_ptrs: bool = False) -> float:
+        """Assembly of the pressure-correction equation (solve_pressure_correction
+        up to the CG, src/mod_pressure_3d.f90:135-310, with apply_pressure_bc,
+        src/mod_boundary_3d.f90:180-277) into the output arrays of ``fields``
+        (an object with the attributes of eafgen.AssemblyFields: float64
+        halo-layout arrays, int32 masks, coordinate arrays, ``flags`` -- 1
+        liquid room valid, 2 gas in the equation, 4 gas compressibility -- and
+        ``scalars`` = (dt, rho_gas, T_ambient, beta_expansion)). Returns the
+        continuity residual sum|Su| / flux_ref."""
+        c = self._assembly_struct(fields)
         res = ctypes.c_double()
         fn = (self._lib.eaf_pressure_assemble_f64_device if device_ptrs
               else self._lib.eaf_pressure_assemble_f64)
         check(fn(self._h, ctypes.byref(c), ctypes.byref(res)), "eaf_pressure_assemble_f64")
         return res.value
+
+    def pressure_step(self, fields, alpha_p: float = 0.7, max_iter: int = MAX_INNER_PRES,
+                      tol: float = SOR_TOL_PRESSURE, device_ptrs: bool = False):
+        """One whole pressure step (src/mod_pressure_3d.f90:135-397): the
+        assembly into ``fields`` (as pressure_assemble), the CG into
+        ``fields.pp``, the post-CG corrections with under-relaxation
+        ``alpha_p`` -- ``fields.p`` and the velocities of the phases in the
+        equation are updated in place. Returns (residual, cg_residual,
+        n_iter, status): the continuity residual (the CG's when that is NaN),
+        the CG's residual and iterations, EAF_OK or EAF_ENONFINITE."""
+        c = self._assembly_struct(fields)
+        res, cres, nit = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        fn = (self._lib.eaf_pressure_step_f64_device if device_ptrs
+              else self._lib.eaf_pressure_step_f64)
+        st = fn(self._h, ctypes.byref(c), float(alpha_p), int(max_iter), float(tol),
+                ctypes.byref(res), ctypes.byref(cres), ctypes.byref(nit))
+        check(st, "eaf_pressure_step_f64", allow=(EAF_OK, EAF_ENONFINITE))
+        return res.value, cres.value, nit.value, st
 
     def solve_mixed(self, arrays, phi, tol: float = SOR_TOL_PRESSURE,
                     inner_tol: float = 0.1, max_outer: int = 200,

@@ -53,6 +53,7 @@ struct eaf_cg {
   double* asm_d;     // assembly mirror: doubles (lazy)
   int* asm_i;        // assembly mirror: ints (lazy)
   double* asm_s;     // assembly scratch: gradients, partials, residual (lazy)
+  cudaEvent_t step_ev[2];  // span of a whole pressure step (lazy)
 };
 
 namespace eaf {
@@ -109,6 +110,8 @@ static void free_handle(eaf_cg* h) {
   cudaFree(h->asm_d);
   cudaFree(h->asm_i);
   cudaFree(h->asm_s);
+  for (int i = 0; i < 2; ++i)
+    if (h->step_ev[i]) cudaEventDestroy(h->step_ev[i]);
   if (h->res_h) cudaFreeHost(h->res_h);
   for (int i = 0; i < 6; ++i)
     if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -593,6 +596,158 @@ int run_assemble(eaf_cg* h, const eaf_assembly_fields_t& f) {
   return EAF_OK;
 }
 
+// Uploads the inputs the switches read into the handle's assembly mirror
+// (allocated on first use) and points d at the mirror: mirror slots 0 vol,
+// 1-3 Ar Ath Az, 4 p, 5 liq_room, 6-13 liquid state, 14 liq_T, 15-22 gas
+// state, 23 gas_T_old, 24-41 outputs (aW .. Fc_z), then the coordinates;
+// ints: cell_type, outlet, act_l, act_g, lk_r, lk_th, lk_z.
+int stage_assembly(eaf_cg* h, const eaf_assembly_fields_t& src, eaf_assembly_fields_t& d) {
+  const size_t nh = h->nh;
+  const size_t nc = (size_t)(h->nr + 4) + (h->nth + 4) + (h->nz + 4);
+  if (!h->asm_d) {
+    EAF_CUDA(cudaMalloc((void**)&h->asm_d, sizeof(double) * ((kAsmIn + kAsmOut) * nh + nc)));
+  }
+  if (!h->asm_i) {
+    EAF_CUDA(cudaMalloc((void**)&h->asm_i, sizeof(int) * kAsmInts * nh));
+  }
+  d = src;
+  auto slot = [&](int i) { return h->asm_d + (size_t)i * nh; };
+  const double* in[kAsmIn] = {src.vol, src.Ar, src.Ath, src.Az, src.p, src.liq_room,
+                              src.liq.alpha, src.liq.rho, src.liq.ur, src.liq.uth,
+                              src.liq.uz, src.liq.aP_ur, src.liq.aP_uth, src.liq.aP_uz,
+                              src.liq_T,
+                              src.gas.alpha, src.gas.rho, src.gas.ur, src.gas.uth,
+                              src.gas.uz, src.gas.aP_ur, src.gas.aP_uth, src.gas.aP_uz,
+                              src.gas_T_old};
+  const double** din[kAsmIn] = {&d.vol, &d.Ar, &d.Ath, &d.Az, &d.p, &d.liq_room,
+                                &d.liq.alpha, &d.liq.rho, &d.liq.ur, &d.liq.uth,
+                                &d.liq.uz, &d.liq.aP_ur, &d.liq.aP_uth, &d.liq.aP_uz,
+                                &d.liq_T,
+                                &d.gas.alpha, &d.gas.rho, &d.gas.ur, &d.gas.uth,
+                                &d.gas.uz, &d.gas.aP_ur, &d.gas.aP_uth, &d.gas.aP_uz,
+                                &d.gas_T_old};
+  for (int i = 0; i < kAsmIn; ++i) {
+    if (!in[i]) continue;  // not read under these switches
+    EAF_CUDA(cudaMemcpyAsync(slot(i), in[i], nh * sizeof(double), cudaMemcpyHostToDevice,
+                             h->st));
+    *din[i] = slot(i);
+  }
+  double* coords = slot(kAsmIn + kAsmOut);
+  EAF_CUDA(cudaMemcpyAsync(coords, src.r, (h->nr + 4) * sizeof(double),
+                           cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4, src.theta, (h->nth + 4) * sizeof(double),
+                           cudaMemcpyHostToDevice, h->st));
+  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4 + h->nth + 4, src.z,
+                           (h->nz + 4) * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  d.r = coords;
+  d.theta = coords + h->nr + 4;
+  d.z = coords + h->nr + 4 + h->nth + 4;
+  const int* in_i[4] = {src.cell_type, src.outlet, src.act_l, src.act_g};
+  const int** din_i[4] = {&d.cell_type, &d.outlet, &d.act_l, &d.act_g};
+  for (int i = 0; i < 4; ++i) {
+    EAF_CUDA(cudaMemcpyAsync(h->asm_i + (size_t)i * nh, in_i[i], nh * sizeof(int),
+                             cudaMemcpyHostToDevice, h->st));
+    *din_i[i] = h->asm_i + (size_t)i * nh;
+  }
+  double** dout[kAsmOut] = {&d.aW, &d.aE, &d.aS, &d.aN, &d.aB, &d.aT, &d.aP, &d.Su, &d.pp,
+                            &d.Fs_r, &d.Fs_th, &d.Fs_z, &d.ac_r, &d.ac_th, &d.ac_z,
+                            &d.Fc_r, &d.Fc_th, &d.Fc_z};
+  for (int i = 0; i < kAsmOut; ++i) *dout[i] = slot(kAsmIn + i);
+  d.lk_r = h->asm_i + 4 * nh;
+  d.lk_th = h->asm_i + 5 * nh;
+  d.lk_z = h->asm_i + 6 * nh;
+  return EAF_OK;
+}
+
+// Downloads the assembly's outputs from the mirror; with `step`, also the
+// arrays the post-CG corrections update (p and the velocities of the phases
+// in the equation).
+int fetch_assembly(eaf_cg* h, const eaf_assembly_fields_t& src, const eaf_assembly_fields_t& d,
+                   bool step) {
+  const size_t bytes = h->nh * sizeof(double);
+  double* out_h[kAsmOut] = {src.aW, src.aE, src.aS, src.aN, src.aB, src.aT, src.aP,
+                            src.Su, src.pp, src.Fs_r, src.Fs_th, src.Fs_z,
+                            src.ac_r, src.ac_th, src.ac_z, src.Fc_r, src.Fc_th, src.Fc_z};
+  const double* out_d[kAsmOut] = {d.aW, d.aE, d.aS, d.aN, d.aB, d.aT, d.aP, d.Su, d.pp,
+                                  d.Fs_r, d.Fs_th, d.Fs_z, d.ac_r, d.ac_th, d.ac_z,
+                                  d.Fc_r, d.Fc_th, d.Fc_z};
+  for (int i = 0; i < kAsmOut; ++i)
+    EAF_CUDA(cudaMemcpyAsync(out_h[i], out_d[i], bytes, cudaMemcpyDeviceToHost, h->st));
+  int* lk_h[3] = {src.lk_r, src.lk_th, src.lk_z};
+  const int* lk_d[3] = {d.lk_r, d.lk_th, d.lk_z};
+  for (int i = 0; i < 3; ++i)
+    EAF_CUDA(cudaMemcpyAsync(lk_h[i], lk_d[i], h->nh * sizeof(int), cudaMemcpyDeviceToHost,
+                             h->st));
+  if (step) {
+    const double* upd_d[7] = {d.p, d.liq.ur, d.liq.uth, d.liq.uz, d.gas.ur, d.gas.uth,
+                              d.gas.uz};
+    const double* upd_h[7] = {src.p, src.liq.ur, src.liq.uth, src.liq.uz, src.gas.ur,
+                              src.gas.uth, src.gas.uz};
+    const int n = d.gas_in_poisson ? 7 : 4;
+    for (int i = 0; i < n; ++i)
+      EAF_CUDA(cudaMemcpyAsync(const_cast<double*>(upd_h[i]), upd_d[i], bytes,
+                               cudaMemcpyDeviceToHost, h->st));
+  }
+  return EAF_OK;
+}
+
+// The serial numerics of solve_pressure_correction (src/mod_pressure_3d.f90:
+// 135-397) on device arrays, back to back on the handle's stream: the
+// assembly (launch_assemble_f64), the CG on its coefficients into pp
+// (cg_3d_mpi, :316-318), then the post-CG corrections (launch_pcorr_f64)
+// over the same arrays -- p and the velocities are updated in place. As the
+// reference (:320), the corrections run whatever the CG returned, and a NaN
+// CG residual replaces the continuity residual.
+int run_step(eaf_cg* h, const eaf_assembly_fields_t& d, double alpha_p, int max_iter,
+             double tol, double* residual, double* cg_res, int* n_iter) {
+  if (!h->asm_s) {
+    EAF_CUDA(cudaMalloc((void**)&h->asm_s,
+                        sizeof(double) * eaf::assembly_scratch_doubles(h->nr, h->nth, h->nz)));
+  }
+  for (int i = 0; i < 2; ++i)
+    if (!h->step_ev[i]) EAF_CUDA(cudaEventCreate(&h->step_ev[i]));
+  EAF_CUDA(cudaEventRecord(h->step_ev[0], h->st));
+  EAF_CUDA(eaf::launch_assemble_f64(d, h->nr, h->nth, h->nz, h->asm_s, h->st));
+  HaloInputs in = {d.aW, d.aE, d.aS, d.aN, d.aB, d.aT, d.aP, d.Su, d.pp};
+  SolveOpts o = {false, max_iter, 0, tol, 0.0};
+  int rc = enqueue_solve(h, in, d.pp, o);
+  if (rc != EAF_OK) return rc;
+  const int cg_kernels = h->last_kernels;
+  auto mut = [](const double* p) { return const_cast<double*>(p); };
+  eaf_pcorr_fields_t pc = {};
+  pc.pp = d.pp;
+  pc.Fs_r = d.Fs_r; pc.Fs_th = d.Fs_th; pc.Fs_z = d.Fs_z;
+  pc.ac_r = d.ac_r; pc.ac_th = d.ac_th; pc.ac_z = d.ac_z;
+  pc.Fc_r = d.Fc_r; pc.Fc_th = d.Fc_th; pc.Fc_z = d.Fc_z;
+  pc.vol = d.vol;
+  pc.r = d.r; pc.theta = d.theta; pc.z = d.z;
+  pc.p = mut(d.p);
+  pc.liq = eaf_phase_fields_t{d.liq.alpha, d.liq.aP_ur, d.liq.aP_uth, d.liq.aP_uz,
+                              mut(d.liq.ur), mut(d.liq.uth), mut(d.liq.uz)};
+  if (d.gas_in_poisson)
+    pc.gas = eaf_phase_fields_t{d.gas.alpha, d.gas.aP_ur, d.gas.aP_uth, d.gas.aP_uz,
+                                mut(d.gas.ur), mut(d.gas.uth), mut(d.gas.uz)};
+  pc.lk_r = d.lk_r; pc.lk_th = d.lk_th; pc.lk_z = d.lk_z;
+  pc.cell_type = d.cell_type;
+  pc.act_l = d.act_l;
+  pc.act_g = d.act_g;
+  pc.has_gas = d.gas_in_poisson;
+  pc.alpha_p = alpha_p;
+  EAF_CUDA(eaf::launch_pcorr_f64(pc, h->nr, h->nth, h->nz, h->st));
+  EAF_CUDA(cudaEventRecord(h->step_ev[1], h->st));
+  const int st = finish_solve(h, false, cg_res, n_iter, nullptr);  // synchronises
+  if (st != EAF_OK && st != EAF_ENONFINITE) return st;
+  double cont = 0.0;
+  EAF_CUDA(cudaMemcpy(&cont, eaf::assembly_result(h->asm_s, h->nr, h->nth, h->nz),
+                      sizeof(double), cudaMemcpyDeviceToHost));
+  *residual = *cg_res != *cg_res ? *cg_res : cont;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->step_ev[0], h->step_ev[1]) == cudaSuccess)
+    h->last_kernel_ms = ms;
+  h->last_kernels = 4 + cg_kernels + 3;
+  return st;
+}
+
 }  // namespace
 
 extern "C" {
@@ -839,76 +994,13 @@ int eaf_pressure_assemble_f64(eaf_cg_t h, const eaf_assembly_fields_t* f, double
   if (!h || !residual || !assembly_fields_ok(f)) return EAF_EINVAL;
   if (h->nh > (size_t)INT32_MAX) return EAF_EUNSUPPORTED;  // 32-bit element indices
   eaf::DeviceGuard guard(h->device);
-  const size_t nh = h->nh;
-  const size_t nc = (size_t)(h->nr + 4) + (h->nth + 4) + (h->nz + 4);
-  if (!h->asm_d) {
-    EAF_CUDA(cudaMalloc((void**)&h->asm_d, sizeof(double) * ((kAsmIn + kAsmOut) * nh + nc)));
-  }
-  if (!h->asm_i) {
-    EAF_CUDA(cudaMalloc((void**)&h->asm_i, sizeof(int) * kAsmInts * nh));
-  }
   const eaf_assembly_fields_t src = assembly_normalised(*f);
-  eaf_assembly_fields_t d = src;
-  auto slot = [&](int i) { return h->asm_d + (size_t)i * nh; };
-  // mirror slots: 0 vol, 1-3 Ar Ath Az, 4 p, 5 liq_room, 6-13 liquid state,
-  // 14 liq_T, 15-22 gas state, 23 gas_T_old, 24-41 outputs (aW .. Fc_z)
-  const double* in[kAsmIn] = {src.vol, src.Ar, src.Ath, src.Az, src.p, src.liq_room,
-                              src.liq.alpha, src.liq.rho, src.liq.ur, src.liq.uth,
-                              src.liq.uz, src.liq.aP_ur, src.liq.aP_uth, src.liq.aP_uz,
-                              src.liq_T,
-                              src.gas.alpha, src.gas.rho, src.gas.ur, src.gas.uth,
-                              src.gas.uz, src.gas.aP_ur, src.gas.aP_uth, src.gas.aP_uz,
-                              src.gas_T_old};
-  const double** din[kAsmIn] = {&d.vol, &d.Ar, &d.Ath, &d.Az, &d.p, &d.liq_room,
-                                &d.liq.alpha, &d.liq.rho, &d.liq.ur, &d.liq.uth,
-                                &d.liq.uz, &d.liq.aP_ur, &d.liq.aP_uth, &d.liq.aP_uz,
-                                &d.liq_T,
-                                &d.gas.alpha, &d.gas.rho, &d.gas.ur, &d.gas.uth,
-                                &d.gas.uz, &d.gas.aP_ur, &d.gas.aP_uth, &d.gas.aP_uz,
-                                &d.gas_T_old};
+  eaf_assembly_fields_t d;
   EAF_CUDA(cudaEventRecord(h->ev[0], h->st));
-  for (int i = 0; i < kAsmIn; ++i) {
-    if (!in[i]) continue;  // not read under these flags
-    EAF_CUDA(cudaMemcpyAsync(slot(i), in[i], nh * sizeof(double), cudaMemcpyHostToDevice,
-                             h->st));
-    *din[i] = slot(i);
-  }
-  double* coords = slot(kAsmIn + kAsmOut);
-  EAF_CUDA(cudaMemcpyAsync(coords, src.r, (h->nr + 4) * sizeof(double),
-                           cudaMemcpyHostToDevice, h->st));
-  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4, src.theta, (h->nth + 4) * sizeof(double),
-                           cudaMemcpyHostToDevice, h->st));
-  EAF_CUDA(cudaMemcpyAsync(coords + h->nr + 4 + h->nth + 4, src.z,
-                           (h->nz + 4) * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  d.r = coords;
-  d.theta = coords + h->nr + 4;
-  d.z = coords + h->nr + 4 + h->nth + 4;
-  const int* in_i[4] = {src.cell_type, src.outlet, src.act_l, src.act_g};
-  const int** din_i[4] = {&d.cell_type, &d.outlet, &d.act_l, &d.act_g};
-  for (int i = 0; i < 4; ++i) {
-    EAF_CUDA(cudaMemcpyAsync(h->asm_i + (size_t)i * nh, in_i[i], nh * sizeof(int),
-                             cudaMemcpyHostToDevice, h->st));
-    *din_i[i] = h->asm_i + (size_t)i * nh;
-  }
-  double* out_h[kAsmOut] = {src.aW, src.aE, src.aS, src.aN, src.aB, src.aT, src.aP,
-                            src.Su, src.pp, src.Fs_r, src.Fs_th, src.Fs_z,
-                            src.ac_r, src.ac_th, src.ac_z, src.Fc_r, src.Fc_th, src.Fc_z};
-  double** dout[kAsmOut] = {&d.aW, &d.aE, &d.aS, &d.aN, &d.aB, &d.aT, &d.aP, &d.Su, &d.pp,
-                            &d.Fs_r, &d.Fs_th, &d.Fs_z, &d.ac_r, &d.ac_th, &d.ac_z,
-                            &d.Fc_r, &d.Fc_th, &d.Fc_z};
-  for (int i = 0; i < kAsmOut; ++i) *dout[i] = slot(kAsmIn + i);
-  d.lk_r = h->asm_i + 4 * nh;
-  d.lk_th = h->asm_i + 5 * nh;
-  d.lk_z = h->asm_i + 6 * nh;
-  int rc = run_assemble(h, d);
+  int rc = stage_assembly(h, src, d);
+  if (rc == EAF_OK) rc = run_assemble(h, d);
+  if (rc == EAF_OK) rc = fetch_assembly(h, src, d, false);
   if (rc != EAF_OK) return rc;
-  for (int i = 0; i < kAsmOut; ++i)
-    EAF_CUDA(cudaMemcpyAsync(out_h[i], *dout[i], nh * sizeof(double), cudaMemcpyDeviceToHost,
-                             h->st));
-  int* lk_h[3] = {src.lk_r, src.lk_th, src.lk_z};
-  for (int i = 0; i < 3; ++i)
-    EAF_CUDA(cudaMemcpyAsync(lk_h[i], h->asm_i + (size_t)(4 + i) * nh, nh * sizeof(int),
-                             cudaMemcpyDeviceToHost, h->st));
   EAF_CUDA(cudaEventRecord(h->ev[5], h->st));
   EAF_CUDA(cudaStreamSynchronize(h->st));
   *residual = h->res_h->residual;
@@ -916,6 +1008,38 @@ int eaf_pressure_assemble_f64(eaf_cg_t h, const eaf_assembly_fields_t* f, double
   if (cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]) == cudaSuccess) h->last_kernel_ms = ms;
   if (cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]) == cudaSuccess) h->last_e2e_ms = ms;
   return EAF_OK;
+}
+
+int eaf_pressure_step_f64_device(eaf_cg_t h, const eaf_assembly_fields_t* f, double alpha_p,
+                                 int max_iter, double tol, double* residual, double* cg_res,
+                                 int* n_iter) {
+  if (!h || !residual || !cg_res || !n_iter || !assembly_fields_ok(f)) return EAF_EINVAL;
+  if (h->nh > (size_t)INT32_MAX) return EAF_EUNSUPPORTED;
+  eaf::DeviceGuard guard(h->device);
+  return run_step(h, assembly_normalised(*f), alpha_p, max_iter, tol, residual, cg_res,
+                  n_iter);
+}
+
+int eaf_pressure_step_f64(eaf_cg_t h, const eaf_assembly_fields_t* f, double alpha_p,
+                          int max_iter, double tol, double* residual, double* cg_res,
+                          int* n_iter) {
+  if (!h || !residual || !cg_res || !n_iter || !assembly_fields_ok(f)) return EAF_EINVAL;
+  if (h->nh > (size_t)INT32_MAX) return EAF_EUNSUPPORTED;
+  eaf::DeviceGuard guard(h->device);
+  const eaf_assembly_fields_t src = assembly_normalised(*f);
+  eaf_assembly_fields_t d;
+  EAF_CUDA(cudaEventRecord(h->ev[0], h->st));
+  int rc = stage_assembly(h, src, d);
+  if (rc != EAF_OK) return rc;
+  const int st = run_step(h, d, alpha_p, max_iter, tol, residual, cg_res, n_iter);
+  if (st != EAF_OK && st != EAF_ENONFINITE) return st;
+  rc = fetch_assembly(h, src, d, true);
+  if (rc != EAF_OK) return rc;
+  EAF_CUDA(cudaEventRecord(h->ev[5], h->st));
+  EAF_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]) == cudaSuccess) h->last_e2e_ms = ms;
+  return st;
 }
 
 }  // extern "C"

@@ -501,6 +501,94 @@ def make_assembly_fields(nr: int, nth: int, nz: int, seed: int = 0, flags: int =
     return f
 
 
+def _wrap_theta(a: np.ndarray) -> None:
+    """Serial theta-periodic halo copy (src/mod_mpi_topology.f90:303-311)."""
+    nth = a.shape[1] - 4
+    a[:, 1] = a[:, nth + 1]
+    a[:, 0] = a[:, nth]
+    a[:, nth + 2] = a[:, 2]
+    a[:, nth + 3] = a[:, 3]
+
+
+def make_pressure_state(nr: int, nth: int, nz: int, seed: int = 0, flags: int = 7,
+                        dt: float = 1e-3) -> AssemblyFields:
+    """A consistent furnace state for one whole pressure step (assembly, CG,
+    post-CG corrections): cylindrical metric arrays of a uniform mesh (cell
+    volume r dr dtheta dz, face areas r_face dtheta dz, dr dz and r dr
+    dtheta, zero at the axis), a steel bath (liquid active, alpha_l ~ 1)
+    under gas, a mixed layer where both phases are active, a few solid cells
+    and sealed cells, electrode holes on the top layer, momentum diagonals
+    that scale with the volume, hydrostatic pressure plus noise. Cells beyond
+    a physical r or z boundary are solid; theta halos are periodic copies of
+    every field, as the reference keeps them. The assembled operator is then
+    symmetric and diagonally dominant, so the CG converges on it. Output
+    arrays start random (the assembly overwrites them)."""
+    rng = np.random.default_rng(seed)
+    shp = halo_shape(nr, nth, nz)
+    dr, dth, dz = R_FURNACE / nr, 2.0 * math.pi / nth, H_FURNACE / nz
+    f = AssemblyFields(nr, nth, nz, flags, [dt, RHO_GAS, 300.0, 1.0e-4])
+    f.r = (np.arange(-1, nr + 3) - 0.5) * dr
+    f.theta = (np.arange(-1, nth + 3) - 0.5) * dth
+    f.z = (np.arange(-1, nz + 3) - 0.5) * dz
+    rc = np.abs(f.r)[None, None, :]
+    rface = np.clip(np.arange(-1, nr + 3), 0, None)[None, None, :] * dr
+    ones = np.ones(shp)
+    f.vol = ones * rc * dr * dth * dz
+    f.Ar = ones * rface * dth * dz
+    f.Ath = ones * dr * dz
+    f.Az = ones * rc * dr * dth
+    zc = f.z[:, None, None] * ones
+    ii = np.arange(-1, nr + 3)[None, None, :] * np.ones(shp, dtype=int)
+    kk = np.arange(-1, nz + 3)[:, None, None] * np.ones(shp, dtype=int)
+    inside = (ii >= 1) & (ii <= nr) & (kk >= 1) & (kk <= nz)
+    f.cell_type = (inside & (rng.random(shp) >= 0.02)).astype(np.int32)
+    bath = 0.3 * H_FURNACE
+    f.act_l = (zc < bath + 2 * dz).astype(np.int32)
+    f.act_g = (zc > bath - 2 * dz).astype(np.int32)
+    sealed = rng.random(shp) < 0.03
+    f.act_l[sealed] = 0
+    f.act_g[sealed] = 0
+    f.liq_alpha = np.clip(0.5 - (zc - bath) / (4 * dz), 0.0, 1.0) * f.act_l
+    f.gas_alpha = (1.0 - f.liq_alpha) * f.act_g
+    f.liq_rho = 7000.0 * rng.uniform(0.98, 1.02, size=shp)
+    f.gas_rho = RHO_GAS * rng.uniform(0.9, 1.1, size=shp)
+    f.liq_T = 1800.0 * rng.uniform(0.98, 1.02, size=shp)
+    f.gas_T_old = rng.uniform(800.0, 2500.0, size=shp)
+    for ph, scale in (("liq", 1e4), ("gas", 1e1)):
+        for c in ("ur", "uth", "uz"):
+            setattr(f, ph + "_" + c, rng.normal(0.0, 0.05, size=shp))
+        for c in ("aP_ur", "aP_uth", "aP_uz"):
+            setattr(f, ph + "_" + c, f.vol * scale * rng.uniform(0.5, 2.0, size=shp) + 1e-12)
+    f.p = 7000.0 * 9.81 * np.clip(bath - zc, 0.0, None) + rng.normal(0.0, 10.0, size=shp)
+    f.liq_room = np.where(rng.random(shp) < 0.05, 5e-5, 1.0)
+    f.outlet = np.zeros(shp, dtype=np.int32)
+    f.outlet[nz + 1][rng.random(shp[1:]) < 0.03] = 1
+    for n in (ASM_DOUBLES_IN[:4] + ("p", "liq_room") + tuple("liq_" + c for c in ASM_PHASE)
+              + tuple("gas_" + c for c in ASM_PHASE) + ("liq_T", "gas_T_old")):
+        _wrap_theta(getattr(f, n))
+    for n in ("cell_type", "outlet", "act_l", "act_g"):
+        _wrap_theta(getattr(f, n))
+    for n in ASM_DOUBLES_OUT:
+        setattr(f, n, rng.normal(size=shp))
+    for n in ("lk_r", "lk_th", "lk_z"):
+        setattr(f, n, rng.integers(0, 3, size=shp).astype(np.int32))
+    return f
+
+
+def pcorr_view(a, alpha_p: float = 0.7) -> PcorrFields:
+    """The post-CG corrections' fields over the SAME arrays (numpy or device
+    tensors) as an assembly's: pp, the exported Fs/ac, Fc and link flags,
+    the mesh, p, the phase states and masks; the gas is in when the
+    assembly's gas-in-equation switch is."""
+    v = PcorrFields(a.nr, a.nth, a.nz, bool(a.flags & 2), alpha_p)
+    for n in PCORR_DOUBLES + PCORR_INTS:
+        setattr(v, n, getattr(a, n))
+    for ph in ("liq", "gas"):
+        for n in PCORR_PHASE:
+            setattr(v, ph + "_" + n, getattr(a, ph + "_" + n))
+    return v
+
+
 def system_bytes(nr: int, nth: int, nz: int) -> int:
     """Host bytes of one system (8 halo-layout FP64 arrays)."""
     return 8 * 8 * (nr + 4) * (nth + 4) * (nz + 4)

@@ -39,6 +39,7 @@ module mod_solver_gpu
     public :: eaf_tdma_3d_f64, eaf_residual_3d_f64
     public :: eaf_phase_fields, eaf_pcorr_fields, pressure_correct_gpu
     public :: eaf_phase_state, eaf_assembly_fields, pressure_assemble_gpu
+    public :: pressure_step_gpu
     public :: cg_3d_gpu_mpi
 
     integer(c_int), parameter, public :: EAF_OK = 0, EAF_ENONFINITE = 3
@@ -211,6 +212,17 @@ module mod_solver_gpu
             type(eaf_assembly_fields), intent(in) :: f
             real(c_double), intent(out) :: residual
         end function eaf_pressure_assemble_f64
+
+        integer(c_int) function eaf_pressure_step_f64(h, f, alpha_p, max_iter, tol, &
+                residual, cg_res, n_iter) bind(C, name="eaf_pressure_step_f64")
+            import :: c_int, c_ptr, c_double, eaf_assembly_fields
+            type(c_ptr), value :: h
+            type(eaf_assembly_fields), intent(in) :: f
+            real(c_double), value :: alpha_p, tol
+            integer(c_int), value :: max_iter
+            real(c_double), intent(out) :: residual, cg_res
+            integer(c_int), intent(out) :: n_iter
+        end function eaf_pressure_step_f64
     end interface
 
     ! One handle per mesh size, kept across SIMPLE iterations like the
@@ -366,6 +378,30 @@ contains
         st = eaf_pressure_assemble_f64(handle, f, residual)
         if (st /= EAF_OK) error stop 'eaf_pressure_assemble_f64 failed'
     end subroutine pressure_assemble_gpu
+
+    ! The serial numerics of solve_pressure_correction (src/mod_pressure_3d.f90:
+    ! 135-397) in one call: pressure_assemble_gpu, the CG into sh%pp
+    ! (cfg%max_inner_pres, SOR_TOL_PRESSURE), then the post-CG corrections with
+    ! cfg%alpha_p over the same arrays -- sh%p and the velocities of the phases
+    ! in the equation are updated in place (f carries c_loc of them). As the
+    ! reference, a NaN cg_res replaces the returned continuity residual.
+    ! Serial meshes only.
+    subroutine pressure_step_gpu(f, m, alpha_p, max_iter, tol, residual, cg_res, n_iter)
+        use mod_types_3d, only: mesh_t
+        type(eaf_assembly_fields), intent(in) :: f
+        type(mesh_t), intent(in) :: m
+        real(c_double), intent(in) :: alpha_p, tol
+        integer, intent(in) :: max_iter
+        real(c_double), intent(out) :: residual, cg_res
+        integer, intent(out) :: n_iter
+        integer(c_int) :: st, nit
+        if (m%is_parallel) error stop 'pressure_step_gpu: decomposed meshes are not supported'
+        call ensure_handle(m%nr, m%ntheta, m%nz)
+        st = eaf_pressure_step_f64(handle, f, alpha_p, int(max_iter, c_int), tol, &
+                                   residual, cg_res, nit)
+        n_iter = int(nit)
+        if (st /= EAF_OK .and. st /= EAF_ENONFINITE) error stop 'eaf_pressure_step_f64 failed'
+    end subroutine pressure_step_gpu
 
     ! Same dummies as cg_3d_mpi for DECOMPOSED meshes (m%is_parallel): the
     ! blocks of the eight coefficient arrays and phi are gathered onto rank 0

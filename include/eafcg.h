@@ -259,6 +259,25 @@ int eaf_pressure_assemble_f64(eaf_cg_t h, const eaf_assembly_fields_t* f, double
 int eaf_pressure_assemble_f64_device(eaf_cg_t h, const eaf_assembly_fields_t* f,
                                      double* residual);
 
+/* One whole pressure step: the serial numerics of solve_pressure_correction
+ * (src/mod_pressure_3d.f90:135-397) -- this assembly, the CG of cg_3d_mpi
+ * into f->pp with max_iter / tol (:316-318), then the post-CG corrections of
+ * eaf_pressure_correct_f64 with under-relaxation alpha_p over the same
+ * arrays (the gas is corrected when gas_in_poisson is set). Besides the
+ * assembly's outputs it updates f->p and the velocities of the phases in the
+ * equation IN PLACE (their pointers are written through). As the reference
+ * (:320), the corrections run whatever the CG returns, and a NaN CG residual
+ * replaces the continuity residual in *residual. *cg_res and *n_iter are the
+ * CG's. Returns the CG's status (EAF_OK or EAF_ENONFINITE) or an error.
+ * Every array is bit-identical to the serial Fortran when the CG's dot
+ * products are associated as the kernel's (eaf_cg_last_launch). */
+int eaf_pressure_step_f64(eaf_cg_t h, const eaf_assembly_fields_t* f, double alpha_p,
+                          int max_iter, double tol, double* residual, double* cg_res,
+                          int* n_iter);
+int eaf_pressure_step_f64_device(eaf_cg_t h, const eaf_assembly_fields_t* f, double alpha_p,
+                                 int max_iter, double tol, double* residual, double* cg_res,
+                                 int* n_iter);
+
 /* Multi-rank drop-in helpers (host-side index work, no device and no MPI):
  * an MPI-decomposed run (m%is_parallel) gathers its blocks onto one rank,
  * solves there on the GPU and scatters the solution back.

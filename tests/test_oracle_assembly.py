@@ -278,3 +278,32 @@ def test_assembly_structure(orc):
     for n in ("aW", "aP", "Su", "pp", "Fs_r", "Fc_z"):
         assert (getattr(f, n)[halo] == 0.0).all()
     assert (f.lk_r[halo] == 0).all()
+
+
+@pytest.mark.parametrize("dims", [(6, 1, 5), (9, 14, 7), (12, 24, 16)])
+def test_consistent_state_assembles_an_spd_operator(dims):
+    """eafgen.make_pressure_state: the assembled operator is symmetric (r and
+    z links exactly; theta links up to the rounding of the seam's centre
+    spacing), weakly diagonally dominant, and the oracle CG solves it; the
+    post-CG corrections run over the same arrays (pcorr_view shares them)."""
+    import oracle
+    g = gen()
+    nr, nth, nz = dims
+    f = g.make_pressure_state(*dims, seed=1)
+    oracle.pressure_assemble(f)
+    I = g.interior
+    aW, aE, aS, aN, aB, aT, aP, Su = [getattr(f, n) for n in g.COEF_NAMES]
+    assert np.array_equal(aE[2:-2, 2:-2, 2:-3], aW[2:-2, 2:-2, 3:-2])
+    assert np.array_equal(aT[2:-3, 2:-2, 2:-2], aB[3:-2, 2:-2, 2:-2])
+    an, as_ = I(aN), I(aS)
+    assert np.allclose(an, np.roll(as_, -1, axis=1), rtol=1e-12, atol=0)
+    off = I(aW) + I(aE) + I(aS) + I(aN) + I(aB) + I(aT)
+    assert (I(aP) >= off).all() and (I(aP) > 0).all()
+    s = g.System(nr=nr, nth=nth, nz=nz, **{n: getattr(f, n) for n in g.COEF_NAMES})
+    res, nit = oracle.cg(s, f.pp, 20000, 1e-8)
+    assert res < 1e-8
+    v = g.pcorr_view(f, 0.7)
+    assert v.pp is f.pp and v.p is f.p and v.liq_ur is f.liq_ur and v.has_gas
+    p0 = f.p.copy()
+    oracle.pressure_correct(v)
+    assert not np.array_equal(f.p, p0)
