@@ -238,6 +238,7 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{dev}")
     torch.cuda.synchronize()
     solver = eaf.CGSolver(nr, nth, nz, device=dev)
+    solver.set_form(CG_FORMS[args.cg_form])
     block, grid = solver.launch()
 
     def one(k, resident=True, host_arrays=None, phi_h=None):
@@ -323,6 +324,7 @@ def run_ours(args, rank, world, local_rank):
                    "mesh": [nr, nth, nz], "cells": n, "spheres": nsph, "tol": TOL,
                    "iterations_per_solve": iters,
                    "launch": {"grid": grid, "block": block},
+                   "cg_form": args.cg_form,
                    "l2": "flushed between steps (256 MiB memset); within a solve "
                          "the ~39 MB symmetric working set is L2-resident",
                    "parallelism": f"replicas x{world} (one furnace per GPU)"},
@@ -374,6 +376,7 @@ def run_fine(args):
     dev = [torch.from_numpy(a).cuda() for a in s.arrays()]
     phi = torch.zeros(g.halo_shape(nr, nth, nz), dtype=torch.float64, device="cuda")
     with eaf.CGSolver(nr, nth, nz) as cg:
+        cg.set_form(CG_FORMS[args.cg_form])
         for _ in range(args.warmup):           # warm-ups capped at 300 iterations
             phi.zero_()
             cg.solve(dev, phi, 300, 0.0, device_ptrs=True)
@@ -404,7 +407,7 @@ def run_fine(args):
                       "cell-iters/s", args.steps, args.warmup, ms / args.steps,
                       "pressure-CG 120x240x168 FP64 cold solves",
                       {"mesh": [nr, nth, nz], "cells": n, "tol": 1e-10,
-                       "iterations_per_solve": its,
+                       "iterations_per_solve": its, "cg_form": args.cg_form,
                        "launch": {"grid": launch[0], "block": launch[1]}})
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_source": f"{kind} hbm_gbs",
@@ -490,6 +493,31 @@ def run_tdma(args):
     return 0
 
 
+def _pinned_fields(eaf, f):
+    """A copy of an eafgen fields object whose arrays live in pinned host
+    memory (the e2e legs upload from page-locked buffers, as a caller that
+    registers its workspace does)."""
+    import numpy as np
+    c = f.copy()
+    for k, v in list(c.__dict__.items()):
+        if isinstance(v, np.ndarray):
+            h = eaf.host_empty(v.shape, v.dtype)
+            h[...] = v
+            setattr(c, k, h)
+    return c
+
+
+def _refill(dst, src) -> None:
+    import numpy as np
+    for k, v in src.__dict__.items():
+        if isinstance(v, np.ndarray):
+            getattr(dst, k)[...] = v
+
+
+# eaf_cg_set_form values
+CG_FORMS = {"reference": 0, "one-reduction": 1}
+DEFAULT_CG_FORM = "reference"
+
 PCORR_BYTES_PER_CELL = 300  # reads 23 doubles + 6 ints, writes 10 doubles (update + sealed pass)
 
 
@@ -526,8 +554,9 @@ def run_pcorr(args):
             kms += cg.last_timing()["kernel_ms"]
         host = f0.copy()
         e2e = 0.0
+        h = _pinned_fields(eaf, f0)
         for _ in range(args.steps):
-            h = f0.copy()
+            _refill(h, f0)
             cg.pressure_correct(h)
             e2e += cg.last_timing()["e2e_ms"]
         cg.pressure_correct(host)
@@ -603,8 +632,9 @@ def run_assemble(args):
             kms += cg.last_timing()["kernel_ms"]
         host = f0.copy()
         e2e = 0.0
+        h = _pinned_fields(eaf, f0)
         for _ in range(args.steps):
-            h = f0.copy()
+            _refill(h, f0)
             cg.pressure_assemble(h)
             e2e += cg.last_timing()["e2e_ms"]
         res = cg.pressure_assemble(host)
@@ -671,6 +701,7 @@ def run_pstep(args):
             getattr(d, k).copy_(v)
 
     with eaf.CGSolver(nr, nth, nz) as cg:
+        cg.set_form(CG_FORMS[args.cg_form])
         for _ in range(args.warmup):
             restore()
             cg.pressure_step(d, alpha_p, max_iter, tol, device_ptrs=True)
@@ -683,8 +714,9 @@ def run_pstep(args):
             kms += cg.last_timing()["kernel_ms"]
             iters.append(nit)
         e2e = 0.0
+        h = _pinned_fields(eaf, f0)
         for _ in range(args.steps):
-            h = f0.copy()
+            _refill(h, f0)
             cg.pressure_step(h, alpha_p, max_iter, tol)
             e2e += cg.last_timing()["e2e_ms"]
         host = f0.copy()
@@ -705,6 +737,7 @@ def run_pstep(args):
                       "post-CG corrections",
                       {"mesh": [nr, nth, nz], "cells": n, "phases": 2, "flags": 7,
                        "cg_tol": tol, "cg_iterations": int(np.median(iters)),
+                       "cg_form": args.cg_form,
                        "l2": "flushed between steps (256 MiB memset)"})
     cg_bytes = 120 * n * float(np.median(iters))
     step_bytes = cg_bytes + ASSEMBLY_BYTES_PER_ELEM * nh + PCORR_BYTES_PER_CELL * n
@@ -863,6 +896,9 @@ def main(argv=None):
     ap.add_argument("--workload", choices=["production", "fine", "batch", "serve", "tdma",
                                            "pcorr", "assemble", "pstep"],
                     default="production")
+    ap.add_argument("--cg-form", choices=sorted(CG_FORMS), default=DEFAULT_CG_FORM,
+                    help="FP64 CG recurrences: the reference's (two all-reduces per "
+                         "iteration) or the single-reduction rearrangement")
     ap.add_argument("--mixed-outer", type=int, default=30)
     ap.add_argument("--mixed-inner", type=int, default=3000)
     ap.add_argument("--rates", default="5,20,50,200")

@@ -262,6 +262,20 @@ class CGSolver:
         check(self._lib.eaf_cg_last_launch(self._h, ctypes.byref(b), ctypes.byref(g)))
         return g.value, b.value
 
+    FORM_REFERENCE = 0
+    FORM_ONE_REDUCTION = 1
+
+    def set_form(self, form: int) -> None:
+        """Recurrences of the plain FP64 solve: FORM_REFERENCE (the
+        reference's PCG, two all-reduces per iteration) or FORM_ONE_REDUCTION
+        (Chronopoulos-Gear, one all-reduce per iteration)."""
+        check(self._lib.eaf_cg_set_form(self._h, int(form)), "set_form")
+
+    def form(self) -> int:
+        f = ctypes.c_int()
+        check(self._lib.eaf_cg_get_form(self._h, ctypes.byref(f)), "get_form")
+        return f.value
+
     def set_timeout_ms(self, ms: float) -> None:
         check(self._lib.eaf_cg_set_timeout_ms(self._h, float(ms)), "set_timeout")
 

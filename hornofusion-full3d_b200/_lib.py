@@ -111,6 +111,8 @@ SIGNATURES = [
     ("eaf_pressure_correct_f64_device", _ci, [_vp, _vp]),
     ("eaf_pressure_assemble_f64", _ci, [_vp, _vp, _pd]),
     ("eaf_pressure_assemble_f64_device", _ci, [_vp, _vp, _pd]),
+    ("eaf_cg_set_form", _ci, [_vp, _ci]),
+    ("eaf_cg_get_form", _ci, [_vp, _pi]),
     ("eaf_pressure_step_f64", _ci, [_vp, _vp, _cd, _ci, _cd, _pd, _pd, _pi]),
     ("eaf_pressure_step_f64_device", _ci, [_vp, _vp, _cd, _ci, _cd, _pd, _pd, _pi]),
     ("eaf_residual_3d_f64_device", _ci, [_vp] + _A8 + [_vp, _pd]),

@@ -50,6 +50,7 @@ struct eaf_cg {
   double* tdma_fac;  // TDMA line factors (lazy)
   double* pc_d;      // post-CG correction mirror: doubles (lazy)
   int* pc_i;         // post-CG correction mirror: ints (lazy)
+  int form;          // EAF_CG_FORM_*: the FP64 solver's recurrences
   double* asm_d;     // assembly mirror: doubles (lazy)
   int* asm_i;        // assembly mirror: ints (lazy)
   double* asm_s;     // assembly scratch: gradients, partials, residual (lazy)
@@ -93,7 +94,8 @@ using eaf::set_error;
 static void free_handle(eaf_cg* h) {
   for (int i = 0; i < 9; ++i) cudaFree(h->stage[i]);
   double* f64[] = {h->s.aP, h->s.aE, h->s.aN, h->s.aT, h->s.aW, h->s.aS, h->s.aB,
-                   h->s.b,  h->s.x,  h->s.r,  h->s.p,  h->s.q,  h->s.p2, h->s.z};
+                   h->s.b,  h->s.x,  h->s.r,  h->s.p,  h->s.q,  h->s.p2, h->s.z,
+                   h->s.s0, h->s.s1, h->s.dinv};
   for (double* p : f64) cudaFree(p);
   cudaFree(h->s.asym);
   float* f32[] = {h->f.aP, h->f.aE, h->f.aN, h->f.aT, h->f.aW, h->f.aS, h->f.aB,
@@ -133,7 +135,9 @@ static int max_coresident(const void* kernel, int block, int sms) {
 // blocks of that size.
 static void pick_launch(const eaf_cg* h, bool f64, int* grid, int* block) {
   auto kernel_for = [f64, h](int b) {
-    return f64 ? eaf::cg_f64_kernel_ptr(b, h->d.n) : eaf::cg_mixed_kernel_ptr();
+    if (!f64) return eaf::cg_mixed_kernel_ptr();
+    return h->form == EAF_CG_FORM_ONE_REDUCTION ? eaf::cg1_f64_kernel_ptr(b)
+                                                : eaf::cg_f64_kernel_ptr(b, h->d.n);
   };
   int b = h->block > 0 ? h->block : kDefaultBlock;
   int g;
@@ -213,7 +217,8 @@ int eaf_cg_create_mesh(eaf_cg_t* out, int nr, int nth, int nz, int is_parallel,
   for (int i = 0; i < 9; ++i) alloc((void**)&h->stage[i], h->nh * sizeof(double));
   double** f64[] = {&h->s.aP, &h->s.aE, &h->s.aN, &h->s.aT, &h->s.aW,
                     &h->s.aS, &h->s.aB, &h->s.b,  &h->s.x,  &h->s.r,
-                    &h->s.p,  &h->s.q,  &h->s.p2, &h->s.z};
+                    &h->s.p,  &h->s.q,  &h->s.p2, &h->s.z, &h->s.s0, &h->s.s1,
+                    &h->s.dinv};
   for (double** p : f64) alloc((void**)p, (size_t)n * sizeof(double));
   alloc((void**)&h->s.asym, sizeof(int));
   int dev_sms = 0;
@@ -272,6 +277,19 @@ int eaf_cg_last_launch(eaf_cg_t h, int* block_threads, int* grid_blocks) {
   if (!h || !block_threads || !grid_blocks) return EAF_EINVAL;
   *block_threads = h->last_block;
   *grid_blocks = h->last_grid;
+  return EAF_OK;
+}
+
+int eaf_cg_set_form(eaf_cg_t h, int form) {
+  if (!h || (form != EAF_CG_FORM_REFERENCE && form != EAF_CG_FORM_ONE_REDUCTION))
+    return EAF_EINVAL;
+  h->form = form;
+  return EAF_OK;
+}
+
+int eaf_cg_get_form(eaf_cg_t h, int* form) {
+  if (!h || !form) return EAF_EINVAL;
+  *form = h->form;
   return EAF_OK;
 }
 
@@ -373,8 +391,12 @@ int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts&
   } else {
     pick_launch(h, true, &grid, &block);
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
-    EAF_CUDA(eaf::launch_cg_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
-                                grid, block, h->st));
+    if (h->form == EAF_CG_FORM_ONE_REDUCTION)
+      EAF_CUDA(eaf::launch_cg1_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
+                                   grid, block, h->st));
+    else
+      EAF_CUDA(eaf::launch_cg_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
+                                  grid, block, h->st));
   }
   h->last_grid = grid;
   h->last_block = block;

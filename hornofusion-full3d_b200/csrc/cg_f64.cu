@@ -275,6 +275,190 @@ __global__ void __launch_bounds__(MAXB, 1) cg_f64_kernel(CgArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Single-reduction form (Chronopoulos and Gear, J. Comput. Appl. Math. 25,
+// 1989): the same preconditioned CG with its recurrences rearranged so that an
+// iteration is ONE phase closed by ONE group all-reduce of three sums:
+//   own cells: u = r dinv, p = u + beta p, s = w + beta s,
+//   x += alpha p, r' = r - alpha s, u' = r' dinv, w' = A u'
+//   (dinv = 1 / max(|aP|, SMALL), stored by the preamble: the Jacobi step is
+//   a multiply here, not the reference's division)
+//   (the six neighbours' u' formed here from their stored r, w and s, final
+//   since the last barrier), partial r'.u', w'.u', r'.r'  -> all-reduce
+// then beta = gamma / max(gamma_prev, SMALL), p.q = delta - beta gamma /
+// alpha_prev, alpha = gamma / p.q, evaluated by every block. r, w and s are
+// double-buffered (neighbours read the old ones while owners write the new);
+// p and x are own-cell only. Iteration 1 takes p = u and s = w exactly. The
+// exit tests, the preconditioner, the stencil's expression order and the NaN
+// outcome are the reference's; the partial table alternates between two slot
+// sets so that a block's next partials never overwrite ones a slower block
+// is still folding. Parity: bit for bit with the oracle's restatement of
+// this form in the kernels' association (eaf_oracle_cg1); against the
+// reference's recurrences, the same residual ball.
+template <bool SYM, int U>
+__device__ void cg1_body(const CgArgs& a, Group& g) {
+  const MeshDims& d = a.d;
+  const SysF64& s = a.s;
+  const Slice own = own_slice(d.n, g.nb, g.bid);
+  const Coefs<double> A = coefs_of<double>(s.aP, s.aE, s.aN, s.aT, s.aW, s.aS, s.aB);
+  const double* __restrict__ aP = s.aP;
+  const double* __restrict__ b = s.b;
+  double* __restrict__ x = s.x;
+  double* __restrict__ p = s.p;
+  const int B = blockDim.x;
+  const int last = own.end - 1;
+
+  // Preamble: dinv = 1 / max(|aP|, SMALL) stored, u0 = r0 * dinv,
+  // w0 = A u0; b.b, r.r, r.u, w.u.
+  double v4[4] = {0.0, 0.0, 0.0, 0.0};
+  double* __restrict__ dinv = s.dinv;
+  {
+    const double* __restrict__ r0 = s.r;
+    double* __restrict__ w0 = s.q;
+    auto u0 = [r0, aP](int cc) { return r0[cc] * (1.0 / guard_small(fabs(aP[cc]))); };
+    for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * U) {
+      double bv[U], rv[U], uv[U], wv[U], iv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int c = min(c0 + u * B, last);
+        bv[u] = b[c];
+        rv[u] = r0[c];
+        iv[u] = 1.0 / guard_small(fabs(aP[c]));
+        uv[u] = rv[u] * iv[u];
+        wv[u] = apply_row_with<SYM, double>(d, A, uv[u], u0, c);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool live = c0 + u * B < own.end;
+        if (live) {
+          w0[c0 + u * B] = wv[u];
+          dinv[c0 + u * B] = iv[u];
+        }
+        v4[0] = v4[0] + (live ? bv[u] * bv[u] : 0.0);
+        v4[1] = v4[1] + (live ? rv[u] * rv[u] : 0.0);
+        v4[2] = v4[2] + (live ? rv[u] * uv[u] : 0.0);
+        v4[3] = v4[3] + (live ? wv[u] * uv[u] : 0.0);
+      }
+    }
+  }
+  bool ok = group_allsum<4>(v4, g, 0);
+  const double bnorm = sqrt(v4[0]);
+  double residual = 0.0;
+  int n_iter = 0;
+  bool nan_fill = false;
+  if (ok && !(bnorm < kSmall)) {
+    double gam = v4[2], dlt = v4[3], gam_prev = 0.0, alpha_prev = 0.0;
+    residual = sqrt(v4[1]) / bnorm;
+    if (residual != residual && a.max_iter >= 1) nan_fill = true;
+    for (int iter = 1; iter <= a.max_iter && !nan_fill; ++iter) {
+      const bool first = iter == 1;
+      double beta = 0.0, den;
+      if (first) {
+        den = dlt;
+      } else {
+        beta = gam / guard_small(gam_prev);
+        den = dlt - beta * gam / alpha_prev;
+      }
+      if (fabs(den) < kSmall) break;
+      const double alpha = gam / den;
+      // buffers: r in (r, z), w in (q, p2), s in (s0, s1); odd iterations
+      // read the first of each pair
+      const bool odd = (iter & 1) != 0;
+      const double* __restrict__ rc = odd ? s.r : s.z;
+      const double* __restrict__ wc = odd ? s.q : s.p2;
+      const double* __restrict__ sc = odd ? s.s0 : s.s1;
+      double* __restrict__ rn = odd ? s.z : s.r;
+      double* __restrict__ wn = odd ? s.p2 : s.q;
+      double* __restrict__ sn = odd ? s.s1 : s.s0;
+      // a neighbour's new preconditioned residual, from its stored values
+      auto unew = [rc, wc, sc, dinv, first, alpha, beta](int cc) {
+        const double sv = first ? wc[cc] : wc[cc] + beta * sc[cc];
+        const double rv = rc[cc] - alpha * sv;
+        return rv * dinv[cc];
+      };
+      double v3[3] = {0.0, 0.0, 0.0};
+      for (int c0 = own.begin + (int)threadIdx.x; c0 < own.end; c0 += B * U) {
+        double rv[U], wv[U], sv[U], pv[U], xv[U], dv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int c = min(c0 + u * B, last);
+          rv[u] = rc[c];
+          wv[u] = wc[c];
+          sv[u] = first ? 0.0 : sc[c];
+          pv[u] = first ? 0.0 : p[c];
+          xv[u] = x[c];
+          dv[u] = dinv[c];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int c = min(c0 + u * B, last);
+          const bool live = c0 + u * B < own.end;
+          const double g0 = dv[u];
+          const double uo = rv[u] * g0;
+          const double pn = first ? uo : uo + beta * pv[u];
+          const double snv = first ? wv[u] : wv[u] + beta * sv[u];
+          const double xn = xv[u] + alpha * pn;
+          const double rnv = rv[u] - alpha * snv;
+          const double un = rnv * g0;
+          const double wnv = apply_row_with<SYM, double>(d, A, un, unew, c);
+          if (live) {
+            p[c] = pn;
+            sn[c] = snv;
+            x[c] = xn;
+            rn[c] = rnv;
+            wn[c] = wnv;
+          }
+          v3[0] = v3[0] + (live ? rnv * un : 0.0);
+          v3[1] = v3[1] + (live ? wnv * un : 0.0);
+          v3[2] = v3[2] + (live ? rnv * rnv : 0.0);
+        }
+      }
+      if (!(ok = group_allsum<3>(v3, g, (iter & 1) ? 4 : 0))) break;
+      gam_prev = gam;
+      alpha_prev = alpha;
+      gam = v3[0];
+      dlt = v3[1];
+      residual = sqrt(v3[2]) / bnorm;
+      n_iter = iter;
+      if (residual < a.tol) break;
+      if (residual != residual && iter < a.max_iter) { nan_fill = true; break; }
+    }
+    if (nan_fill) {
+      const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+      for (int c = own.begin + (int)threadIdx.x; c < own.end; c += B) x[c] = qnan;
+      residual = qnan;
+      n_iter = a.max_iter;
+    }
+  }
+  if (g.bid == 0 && threadIdx.x == 0) {
+    SolveResult* res = a.ws.result;
+    const int err = ld_volatile_i32(a.ws.err);
+    res->status = err != 0 ? err : (isfinite(residual) ? EAF_OK : EAF_ENONFINITE);
+    res->n_iter = n_iter;
+    res->n_outer = 0;
+    res->sym = SYM ? 1 : 0;
+    res->residual = residual;
+    res->bnorm = bnorm;
+  }
+}
+
+template <int MAXB, int U>
+__global__ void __launch_bounds__(MAXB, 1) cg1_f64_kernel(CgArgs a) {
+  Group g;
+  g.counter = a.ws.counter;
+  g.err = a.ws.err;
+  g.part = a.ws.part;
+  g.stage = group_stage_smem();
+  g.nb = gridDim.x;
+  g.bid = blockIdx.x;
+  g.timeout_ns = a.timeout_ns;
+  g.epoch = 0;
+  if (*a.s.asym == 0)
+    cg1_body<true, U>(a, g);
+  else
+    cg1_body<false, U>(a, g);
+}
+
+// ---------------------------------------------------------------------------
 // Batched launch (see BatchTables): the same solver body per system, on the
 // lane's blocks with the lane's barrier counter and partial table.
 // ---------------------------------------------------------------------------
@@ -470,6 +654,31 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
   void* args[] = {&a};
   return cudaLaunchCooperativeKernel(cg_f64_kernel_ptr(block, d.n), dim3(grid),
                                      dim3(block), args, 0, st);
+}
+
+cudaError_t launch_cg1_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                           int max_iter, double tol, uint64_t timeout_ns, int grid,
+                           int block, cudaStream_t st) {
+  if (!s.s0 || !s.s1) return cudaErrorInvalidValue;
+  CgArgs a;
+  a.d = d;
+  a.s = s;
+  a.ws = ws;
+  a.max_iter = max_iter;
+  a.tol = tol;
+  a.timeout_ns = timeout_ns;
+  cudaError_t e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  void* args[] = {&a};
+  return cudaLaunchCooperativeKernel(cg1_f64_kernel_ptr(block), dim3(grid), dim3(block), args,
+                                     0, st);
+}
+
+const void* cg1_f64_kernel_ptr(int block) {
+  if (block <= 256) return (const void*)cg1_f64_kernel<256, 4>;
+  if (block <= 512) return (const void*)cg1_f64_kernel<512, 2>;
+  return (const void*)cg1_f64_kernel<1024, 1>;
 }
 
 bool l2_prefetch_pays(long long n) { return (double)n * 128.0 > 96.0e6; }

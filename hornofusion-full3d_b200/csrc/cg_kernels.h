@@ -40,6 +40,8 @@ struct SysF64 {
   double *b, *x, *r, *q;
   double *p, *p2;             // search direction, double-buffered by iteration
   double *z;                  // preconditioned residual r / max(|aP|, SMALL)
+  double *s0, *s1;            // single-reduction form: s = A p, double-buffered
+  double *dinv;               // single-reduction form: 1 / max(|aP|, SMALL)
   int* asym;                  // pack: number of link pairs that disagree
 };
 
@@ -81,6 +83,13 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
 // same bits for one launch shape.
 bool l2_prefetch_pays(long long n);
 const void* cg_f64_kernel_ptr(int block, long long n);
+// Single-reduction (Chronopoulos-Gear) form of the same PCG: one group
+// all-reduce per iteration; uses s0/s1 and reuses r, z, q, p2 as the
+// double-buffered r and w = A M^-1 r.
+cudaError_t launch_cg1_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                           int max_iter, double tol, uint64_t timeout_ns, int grid, int block,
+                           cudaStream_t st);
+const void* cg1_f64_kernel_ptr(int block);
 
 
 

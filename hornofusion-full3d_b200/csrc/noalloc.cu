@@ -140,6 +140,7 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
   s.q = base + 11 * M;
   s.p2 = base + 12 * M;
   s.z = base + 13 * M;
+  s.s0 = s.s1 = s.dinv = nullptr;  // the single-reduction form is not launched here
   s.asym = reinterpret_cast<int*>(base + kAsymOff);
   eaf::GroupWs ws;
   ws.part = base + kPartOff;

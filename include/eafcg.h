@@ -314,6 +314,22 @@ int eaf_mr_extract(const double* global, int nr, int nth, int nz, const int loc[
 int eaf_mr_unpack(double* local, int nr, int nz, const int loc[3], const int start[3],
                   const double* buf);
 
+/* Recurrences of the plain FP64 solve on this handle (eaf_cg_solve_f64 and
+ * its _device form, and the CG inside eaf_pressure_step_f64):
+ *   EAF_CG_FORM_REFERENCE      the reference's PCG recurrences
+ *     (src/mod_solver_3d.f90:531-559), two group all-reduces per iteration;
+ *     every per-cell value is the reference's, only the dot association
+ *     differs (bit-identical to the oracle in the kernels' association);
+ *   EAF_CG_FORM_ONE_REDUCTION  the same PCG rearranged (Chronopoulos-Gear)
+ *     so that each iteration has ONE all-reduce; the same preconditioner,
+ *     stencil, exit tests and NaN outcome, different rounding: it reaches the
+ *     same tolerance in a few per cent more or fewer iterations.
+ * No reference counterpart (the reference has one form). */
+#define EAF_CG_FORM_REFERENCE 0
+#define EAF_CG_FORM_ONE_REDUCTION 1
+int eaf_cg_set_form(eaf_cg_t h, int form);
+int eaf_cg_get_form(eaf_cg_t h, int* form);
+
 /* Bound on every device-side barrier wait, in milliseconds (default 2000). */
 int eaf_cg_set_timeout_ms(eaf_cg_t h, double ms);
 

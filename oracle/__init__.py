@@ -41,6 +41,8 @@ def lib():
         L.eaf_oracle_cg_threads.restype = ci
         L.eaf_oracle_cg_tree.argtypes = (L.eaf_oracle_cg.argtypes + [ci, ci])
         L.eaf_oracle_cg_tree.restype = ci
+        L.eaf_oracle_cg1.argtypes = (L.eaf_oracle_cg.argtypes + [ci, ci])
+        L.eaf_oracle_cg1.restype = ci
         L.eaf_oracle_dot.argtypes = [ci, ci, ci, _dp, _dp, ci, ci]
         L.eaf_oracle_dot.restype = cd
         L.eaf_oracle_matvec.argtypes = [ci, ci, ci] + [_dp] * 9
@@ -91,6 +93,22 @@ def cg(system, phi: np.ndarray, max_iter: int, tol: float, nthreads: int = 1,
         rc = lib().eaf_oracle_cg_threads(*args, int(nthreads))
     if rc != 0:
         raise RuntimeError(f"oracle cg failed with status {rc}")
+    return res.value, nit.value
+
+
+def cg1(system, phi: np.ndarray, max_iter: int, tol: float, plan: tuple | None = None):
+    """The single-reduction (Chronopoulos-Gear) form of the same PCG, in
+    place on ``phi``; ``plan=(G, B)`` associates its dots as the CUDA
+    single-reduction kernel does. Returns (residual, n_iter)."""
+    res = ctypes.c_double(0.0)
+    nit = ctypes.c_int(0)
+    G, B = plan if plan is not None else (0, 0)
+    args = [system.nr, system.nth, system.nz] + [_p(a) for a in system.arrays()]
+    args += [_p(phi), int(max_iter), float(tol), ctypes.byref(res), ctypes.byref(nit),
+             int(G), int(B)]
+    rc = lib().eaf_oracle_cg1(*args)
+    if rc != 0:
+        raise RuntimeError(f"oracle cg1 failed with status {rc}")
     return res.value, nit.value
 
 

@@ -362,6 +362,126 @@ int eaf_oracle_cg_tree(int nr, int nth, int nz, const double* aW,
                    tol, residual, n_iter, 1, pl);
 }
 
+/* ----------------------------------------------------------------------
+ * Single-reduction form of the same preconditioned CG (Chronopoulos and
+ * Gear, "s-step iterative methods for symmetric linear systems", J. Comput.
+ * Appl. Math. 25, 1989): the reference's recurrences rearranged so that the
+ * three scalars of an iteration -- gamma = r.u, delta = w.u (u = M^-1 r,
+ * w = A u) and r.r -- come from ONE reduction; s = A p is carried by the
+ * recurrence s = w + beta s, and p.q by delta - beta gamma / alpha_prev.
+ * Not the reference's arithmetic: it lands elsewhere in the residual ball
+ * (test bar: both residuals < tol, iterations within a few per cent), and
+ * the Jacobi step multiplies by 1 / max(|aP|, SMALL) instead of dividing.
+ * The matvec expression order, the exit tests (strict
+ * < tol after the update, breakdown |p.q| < SMALL, beta guard
+ * max(gamma_prev, SMALL)) and the NaN behaviour are the reference's.
+ * First iteration: p = u, s = w exactly. With plan.G > 0 the dots take the
+ * kernels' association: this is the parity oracle of the CUDA
+ * single-reduction kernel, bit for bit.
+ * ---------------------------------------------------------------------- */
+static int cg1_impl(int nr, int nth, int nz, const double* aW, const double* aE,
+                    const double* aS, const double* aN, const double* aB,
+                    const double* aT, const double* aP, const double* Su,
+                    double* phi, int max_iter, double tol, double* residual,
+                    int* n_iter, plan_t plan) {
+    if (nr < 1 || nth < 1 || nz < 1) return 2;
+    if (plan.G < 0 || (plan.G > 0 && plan.B < 1)) return 2;
+    op_t o;
+    o.plan = plan;
+    o.d = mkdims(nr, nth, nz);
+    o.aW = aW; o.aE = aE; o.aS = aS; o.aN = aN; o.aB = aB; o.aT = aT; o.aP = aP;
+    o.nthreads = 1;
+    const dims_t* d = &o.d;
+    double* r = (double*)calloc(d->n, sizeof(double));
+    double* u = (double*)calloc(d->n, sizeof(double));
+    double* w = (double*)calloc(d->n, sizeof(double));
+    double* pv = (double*)calloc(d->n, sizeof(double));
+    double* sv = (double*)calloc(d->n, sizeof(double));
+    if (!r || !u || !w || !pv || !sv) {
+        free(r); free(u); free(w); free(pv); free(sv);
+        return 6;
+    }
+    matvec(&o, phi, w);
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= nth; ++j)
+            for (int i = 1; i <= nr; ++i) {
+                size_t c = at(d, i, j, k);
+                r[c] = Su[c] - w[c];
+            }
+    double bnorm = sqrt(dot(&o, Su, Su));
+    if (bnorm < SMALL) {
+        *residual = 0.0;
+        *n_iter = 0;
+        free(r); free(u); free(w); free(pv); free(sv);
+        return 0;
+    }
+#define PRECOND()                                                       \
+    for (int k = 1; k <= nz; ++k)                                       \
+        for (int j = 1; j <= nth; ++j)                                  \
+            for (int i = 1; i <= nr; ++i) {                             \
+                size_t c = at(d, i, j, k);                              \
+                u[c] = r[c] * (1.0 / guard(fabs(aP[c])));               \
+            }
+    PRECOND();
+    matvec(&o, u, w);
+    double gam = dot(&o, r, u), dlt = dot(&o, w, u);
+    double res = sqrt(dot(&o, r, r)) / bnorm;
+    double alpha_prev = 0.0, gam_prev = 0.0;
+    int nit = 0;
+    for (int iter = 1; iter <= max_iter; ++iter) {
+        double beta = 0.0, den;
+        if (iter == 1) {
+            den = dlt;
+        } else {
+            beta = gam / guard(gam_prev);
+            den = dlt - beta * gam / alpha_prev;
+        }
+        if (fabs(den) < SMALL) break;
+        double alpha = gam / den;
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= nth; ++j)
+                for (int i = 1; i <= nr; ++i) {
+                    size_t c = at(d, i, j, k);
+                    if (iter == 1) {
+                        pv[c] = u[c];
+                        sv[c] = w[c];
+                    } else {
+                        pv[c] = u[c] + beta * pv[c];
+                        sv[c] = w[c] + beta * sv[c];
+                    }
+                    phi[c] = phi[c] + alpha * pv[c];
+                    r[c] = r[c] - alpha * sv[c];
+                }
+        PRECOND();
+        matvec(&o, u, w);
+        gam_prev = gam;
+        alpha_prev = alpha;
+        gam = dot(&o, r, u);
+        dlt = dot(&o, w, u);
+        res = sqrt(dot(&o, r, r)) / bnorm;
+        nit = iter;
+        if (res < tol) break;
+    }
+#undef PRECOND
+    eaf_oracle_theta_wrap(nr, nth, nz, phi);
+    *residual = res;
+    *n_iter = nit;
+    free(r); free(u); free(w); free(pv); free(sv);
+    return 0;
+}
+
+/* Single-reduction CG, sequential dots (G == 0) or the kernels' association
+ * for a launch of G blocks x B threads. Returns 0, 2 or 6. */
+int eaf_oracle_cg1(int nr, int nth, int nz, const double* aW, const double* aE,
+                   const double* aS, const double* aN, const double* aB,
+                   const double* aT, const double* aP, const double* Su,
+                   double* phi, int max_iter, double tol, double* residual,
+                   int* n_iter, int G, int B) {
+    plan_t pl = {G, B};
+    return cg1_impl(nr, nth, nz, aW, aE, aS, aN, aB, aT, aP, Su, phi, max_iter,
+                    tol, residual, n_iter, pl);
+}
+
 /* Interior dot of two halo-layout arrays in the kernels' association
  * (G, B) or, with G == 0, the reference's sequential order. */
 double eaf_oracle_dot(int nr, int nth, int nz, const double* a, const double* b,

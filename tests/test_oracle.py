@@ -297,3 +297,25 @@ def test_kernel_order_solve_agrees_with_sequential_closely(orc):
     orc.cg(s, p2, 60, 0.0, plan=(3, 512))
     I = g.interior
     assert np.linalg.norm(I(p1) - I(p2)) <= 1e-13 * np.linalg.norm(I(p1))
+
+
+@pytest.mark.parametrize("dims,seed", [((12, 24, 16), 0), ((18, 36, 24), 1)])
+def test_single_reduction_form_reaches_the_reference_ball(dims, seed):
+    """oracle.cg1 (Chronopoulos-Gear rearrangement): same tolerance, iteration
+    count within a few per cent of the reference recurrences in the kernels'
+    association, solution within the spread of two correct FP64 CGs."""
+    import oracle
+    g = gen()
+    s = g.make_system(*dims, nsph=8, seed=seed)
+    plan = (8, 256)
+    a = g.zeros_phi(*dims)
+    b = g.zeros_phi(*dims)
+    ra, na = oracle.cg(s, a, 100000, 1e-8, plan=plan)
+    rb, nb = oracle.cg1(s, b, 100000, 1e-8, plan=plan)
+    assert ra < 1e-8 and rb < 1e-8
+    assert abs(na - nb) <= max(2, 0.06 * na), (na, nb)
+    ia, ib = g.interior(a), g.interior(b)
+    assert np.linalg.norm(ia - ib) / np.linalg.norm(ia) < 2e-8
+    # the theta-halo post-condition holds for the new form too
+    nth = dims[1]
+    assert np.array_equal(b[:, 1, :], b[:, nth + 1, :])
