@@ -18,6 +18,17 @@ e2e   : the same chain through the host-pointer C-ABI call (the Fortran
 The reference arm (--impl reference) times the oracle port of the
 reference CG (no Fortran toolchain exists to build the reference itself) on
 all host cores over a bounded sample of the same workload.
+
+Further lines (--workload; one JSON line each, not the headline):
+  fine      120x240x168 FP64 cold solves to 1e-10 and the mixed form
+  batch     96 uneven systems in one persistent launch vs one by one
+  serve     Poisson streams of furnace runs through the serving loop
+  tdma      line-by-line TDMA sweeps of a transport system
+  pcorr     the post-CG corrections of the pressure step
+  assemble  the assembly of the pressure-correction equation
+  pstep     one whole pressure step: assembly, CG, corrections
+--cg-form selects the FP64 CG's recurrences (reference: two all-reduces per
+iteration, the default; one-reduction: the Chronopoulos-Gear form).
 """
 from __future__ import annotations
 
