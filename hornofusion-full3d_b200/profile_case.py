@@ -2,6 +2,7 @@
 
     python hornofusion-full3d_b200/profile_case.py --mesh 60 120 84 \
         --iters 400 [--mixed] [--launch BLOCK GRID] [--repeat R]
+        [--form reference|one-reduction]
 
 Builds the seeded system, uploads it once, then runs R solves through the
 device-pointer C-ABI entry with tol 0 (exactly `--iters` iterations, so the
@@ -24,6 +25,8 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=400)
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--mixed", action="store_true")
+    ap.add_argument("--form", choices=["reference", "one-reduction"], default="reference",
+                    help="recurrences of the plain FP64 solve")
     ap.add_argument("--launch", type=int, nargs=2, default=None)
     ap.add_argument("--batch", type=int, default=0,
                     help="solve this many copies of the mixed batch instead "
@@ -46,6 +49,8 @@ def main(argv=None):
     torch.cuda.synchronize()
     out = []
     with eaf.CGSolver(nr, nth, nz) as cg:
+        cg.set_form(cg.FORM_ONE_REDUCTION if args.form == "one-reduction"
+                    else cg.FORM_REFERENCE)
         if args.launch:
             cg.set_launch(*args.launch)
         block, grid = cg.launch()
