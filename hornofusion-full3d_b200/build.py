@@ -30,6 +30,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
 # Per-unit extra flags.
 UNITS = {
     "api.cu": [],
+    "api_pressure.cu": [],
     "cg_f64.cu": ["-fmad=false"],
     "cg_mixed.cu": [],
     "batch.cu": [],
