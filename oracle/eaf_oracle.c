@@ -47,7 +47,10 @@
  *     (cell_gradients :621-651, add_phase_contribution :469-619, helpers
  *     :405-458, :654-681; pgrad src/mod_constants.f90:274-287;
  *     apply_pressure_bc src/mod_boundary_3d.f90:180-277)
- * (eaf_oracle_pressure_assemble).
+ * (eaf_oracle_pressure_assemble). It also restates the single-reduction
+ * (Chronopoulos-Gear) rearrangement of the same CG that the CUDA library
+ * offers as an option (eaf_oracle_cg1): not reference arithmetic, the
+ * checker of that form only.
  *
  * PARITY UNPINNED: the reference is Fortran + MPI and no Fortran compiler or
  * MPI exists where this is built or run, and the reference's tests pin only
