@@ -98,3 +98,43 @@ def test_step_iteration_cap_still_corrects():
     b, cont, cres_o, nit_o = run_oracle(f, plan, max_iter=7)
     assert nit == nit_o == 7 and cres == cres_o and cres > 1e-8
     assert_step_equal(a, b)
+
+
+@pytest.mark.parametrize("flags", [0, 5])
+def test_step_bitwise_remaining_switches(flags):
+    """No liquid room and no gas (0); compressibility with the gas outside the
+    equation (5: gas alpha, rho and T_old read, no gas face or correction)."""
+    f = gen().make_pressure_state(12, 24, 16, seed=6, flags=flags)
+    a, (res, cres, nit, st), plan, _ = run_gpu(f)
+    b, cont, cres_o, nit_o = run_oracle(f, plan)
+    assert st == 0 and (cres, nit) == (cres_o, nit_o)
+    assert abs(res - cont) <= 1e-12 * abs(cont)
+    assert_step_equal(a, b)
+
+
+def test_step_with_no_cg_iterations_still_corrects():
+    """max_iter 0: the CG leaves pp at the assembly's zeros, and the
+    corrections run on it as the reference's would."""
+    f = gen().make_pressure_state(9, 14, 7, seed=8, flags=7)
+    a, (res, cres, nit, st), plan, _ = run_gpu(f, max_iter=0)
+    b, cont, cres_o, nit_o = run_oracle(f, plan, max_iter=0)
+    assert nit == nit_o == 0 and cres == cres_o
+    assert not a.pp.any()
+    assert_step_equal(a, b)
+
+
+def test_step_argument_errors():
+    eaf = pkg()
+    f = gen().make_pressure_state(6, 8, 5, seed=1, flags=7)
+    with eaf.CGSolver(6, 8, 5) as cg:
+        bad = f.copy()
+        bad.gas_uz = None
+        with pytest.raises(eaf.EafError):
+            cg.pressure_step(bad, ALPHA_P, 100, 1e-8)
+        bad = f.copy()
+        bad.scalars[0] = -1.0
+        with pytest.raises(eaf.EafError):
+            cg.pressure_step(bad, ALPHA_P, 100, 1e-8)
+        # the handle stays usable after refused calls
+        r = cg.pressure_step(f.copy(), ALPHA_P, 20000, 1e-8)
+        assert r[3] == 0
