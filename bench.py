@@ -27,6 +27,10 @@ Further lines (--workload; one JSON line each, not the headline):
   pcorr     the post-CG corrections of the pressure step
   assemble  the assembly of the pressure-correction equation
   pstep     one whole pressure step: assembly, CG, corrections
+  fixed     a fixed amount of work for profiling and per-iteration timing:
+            --repeat solves of exactly --iters CG iterations on --mesh
+            (tol 0), or --batch-size systems of the batch mix, or
+            --tdma-sweeps sweeps with --fixed-tdma
 --cg-form selects the FP64 CG's recurrences (reference: two all-reduces per
 iteration, the default; one-reduction: the Chronopoulos-Gear form).
 """
@@ -895,6 +899,83 @@ def run_serve(args):
     return 0
 
 
+def run_fixed(args):
+    """A fixed amount of work per launch, for ncu captures and per-iteration
+    timing: the seeded system of --mesh uploaded once, then --repeat solves
+    of exactly --iters iterations (tol 0) through the device-pointer entry;
+    or --batch-size systems of the batch mix (round robin) at --iters
+    iterations each; or --tdma-sweeps sweeps of a transport system
+    (--fixed-tdma)."""
+    import torch
+    eaf = importlib.import_module(PKG)
+    g = importlib.import_module(PKG + ".eafgen")
+    nr, nth, nz = args.mesh
+    runs = []
+    if args.batch_size:
+        meshes = [d for d, _ in g.BATCH_MIX]
+        systems = [g.make_system(*meshes[k % len(meshes)], seed=k)
+                   for k in range(args.batch_size)]
+        dims = [(s.nr, s.nth, s.nz) for s in systems]
+        dev = [[torch.from_numpy(a).cuda() for a in s.arrays()] for s in systems]
+        phis = [torch.zeros(g.halo_shape(*d), dtype=torch.float64, device="cuda")
+                for d in dims]
+        cells = sum(d[0] * d[1] * d[2] for d in dims)
+        with eaf.Batch(dims) as b:
+            for i in range(len(systems)):
+                b.set_system(i, dev[i], phis[i], device_ptrs=True)
+            for _ in range(args.repeat):
+                for p in phis:
+                    p.zero_()
+                torch.cuda.synchronize()
+                b.solve(max_iter=args.iters, tol=0.0)
+                runs.append({"batch_ms": b.last_ms,
+                             "cell_iters_per_s": cells * args.iters / (b.last_ms / 1e3)})
+            launch = list(b.plan())
+        case = {"batch": dims}
+    elif args.fixed_tdma:
+        s = g.make_transport_system(nr, nth, nz, seed=0)
+        dev = [torch.from_numpy(a).cuda() for a in s.arrays()]
+        phi = torch.zeros(g.halo_shape(nr, nth, nz), dtype=torch.float64, device="cuda")
+        with eaf.CGSolver(nr, nth, nz) as cg:
+            for _ in range(args.repeat):
+                phi.zero_()
+                torch.cuda.synchronize()
+                cg.tdma(dev, phi, args.tdma_sweeps, device_ptrs=True)
+                t = cg.last_timing()
+                runs.append({"sweeps": args.tdma_sweeps, "kernel_ms": t["kernel_ms"],
+                             "ms_per_sweep": t["kernel_ms"] / args.tdma_sweeps})
+            launch = list(cg.last_launch())
+        case = {"mesh": [nr, nth, nz], "tdma": True}
+    else:
+        s = g.make_system(nr, nth, nz, args.spheres, seed=0)
+        dev = [torch.from_numpy(a).cuda() for a in s.arrays()]
+        phi = torch.zeros(g.halo_shape(nr, nth, nz), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        with eaf.CGSolver(nr, nth, nz) as cg:
+            cg.set_form(CG_FORMS[args.cg_form])
+            if args.launch:
+                cg.set_launch(*args.launch)
+            for _ in range(args.repeat):
+                phi.zero_()
+                torch.cuda.synchronize()
+                if args.mixed:
+                    res, nit, nout, st = cg.solve_mixed(
+                        dev, phi, tol=0.0, inner_tol=1e-30, max_outer=1,
+                        max_inner=args.iters, device_ptrs=True)
+                else:
+                    res, nit, st = cg.solve(dev, phi, args.iters, 0.0, device_ptrs=True)
+                t = cg.last_timing()
+                runs.append({"iters": nit, "residual": res, "status": st,
+                             "kernel_ms": t["kernel_ms"], "solve_ms": t["solve_ms"],
+                             "us_per_iter": 1e3 * t["kernel_ms"] / max(nit, 1)})
+            launch = list(cg.last_launch())
+        case = {"mesh": [nr, nth, nz], "iters": args.iters, "mixed": args.mixed,
+                "cg_form": args.cg_form}
+    print(json.dumps({"workload": "fixed", "case": case, "launch": launch, "runs": runs}),
+          flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -905,7 +986,7 @@ def main(argv=None):
                     help="iteration cap per reference-arm step (bounded sample)")
     ap.add_argument("--tdma-sweeps", type=int, default=3)
     ap.add_argument("--workload", choices=["production", "fine", "batch", "serve", "tdma",
-                                           "pcorr", "assemble", "pstep"],
+                                           "pcorr", "assemble", "pstep", "fixed"],
                     default="production")
     ap.add_argument("--cg-form", choices=sorted(CG_FORMS), default=DEFAULT_CG_FORM,
                     help="FP64 CG recurrences: the reference's (two all-reduces per "
@@ -916,11 +997,21 @@ def main(argv=None):
     ap.add_argument("--serve-runs", type=int, default=25)
     ap.add_argument("--solves-per-run", type=int, default=50)
     ap.add_argument("--serve-mixed", action="store_true")
+    # --workload fixed
+    ap.add_argument("--mesh", type=int, nargs=3, default=list(MESH[:3]))
+    ap.add_argument("--spheres", type=int, default=MESH[3])
+    ap.add_argument("--iters", type=int, default=400)
+    ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--launch", type=int, nargs=2, default=None, metavar=("BLOCK", "GRID"))
+    ap.add_argument("--mixed", action="store_true")
+    ap.add_argument("--batch-size", type=int, default=0)
+    ap.add_argument("--fixed-tdma", action="store_true")
     args = ap.parse_args(argv)
     if args.workload != "production" and args.impl == "ours":
         return {"fine": run_fine, "batch": run_batch, "serve": run_serve,
                 "tdma": run_tdma, "pcorr": run_pcorr,
-                "assemble": run_assemble, "pstep": run_pstep}[args.workload](args)
+                "assemble": run_assemble, "pstep": run_pstep,
+                "fixed": run_fixed}[args.workload](args)
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local_rank = _env_int("LOCAL_RANK", 0)

@@ -172,7 +172,7 @@ struct TunedWidth {{
 }};
 
 // Lane width (blocks of 512 threads) of batched and served solves.
-static const TunedWidth kTunedWidths[] = {{
+static constexpr TunedWidth kTunedWidths[] = {{
 {rows_l}
 }};
 
@@ -189,9 +189,17 @@ struct TunedLaunch {{
 }};
 
 // (block, grid) of the single-system persistent solver.
-static const TunedLaunch kTunedLaunches[] = {{
+static constexpr TunedLaunch kTunedLaunches[] = {{
 {rows_s}
 }};
+
+// Largest tuned grid among meshes of at most `max_cells` cells (0 if none).
+constexpr int max_tuned_grid_up_to(long long max_cells) {{
+  int g = 0;
+  for (const TunedLaunch& t : kTunedLaunches)
+    if ((long long)t.nr * t.nth * t.nz <= max_cells && t.grid > g) g = t.grid;
+  return g;
+}}
 
 inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid) {{
   for (const TunedLaunch& t : kTunedLaunches)

@@ -20,9 +20,10 @@
 //     or different streams not ordered by the caller) race on the array.
 //     Callers serialise their calls per device;
 //   * the first call on a device looks the array's device address up with
-//     cudaGetSymbolAddress (once per device, with that device current). That
-//     first call should therefore come before any stream capture begins on
-//     the device.
+//     cudaGetSymbolAddress (with that device current) and keeps it for the
+//     later calls; a lookup that fails is not kept, so the next call tries
+//     again. That first call should come before any stream capture begins
+//     on the device.
 // The kernels are the ones eaf_cg_solve_f64_device runs (pack, persistent
 // cooperative CG, unpack), launched with the same default shape, so results
 // are bit-identical to that entry point on the same inputs.
@@ -40,7 +41,17 @@
 namespace {
 
 constexpr int kNoallocMaxCells = EAF_NOALLOC_MAX_CELLS;
+// Blocks of the largest launch this entry makes; the partial table is sized
+// for it. Every launch shape the handle entries pick for a mesh of at most
+// kNoallocMaxCells cells must fit, or the two would not give the same bits:
+// the tuned shapes (checked here) and the fallback of one 512-thread block
+// per 2048 cells.
 constexpr int kNoallocMaxBlocks = 64;
+static_assert(eaf::max_tuned_grid_up_to(kNoallocMaxCells) <= kNoallocMaxBlocks,
+              "a tuned launch for a mesh within the no-allocation limit has more "
+              "blocks than the static scratch holds partials for");
+static_assert((kNoallocMaxCells + 2047) / 2048 <= kNoallocMaxBlocks,
+              "the fallback launch shape exceeds the static scratch's block limit");
 constexpr int kPartSlots = 8;
 constexpr int kMaxDevices = 64;
 constexpr uint64_t kNoallocTimeoutNs = 2000ull * 1000ull * 1000ull;
@@ -61,22 +72,27 @@ constexpr size_t kScratchDoubles =
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 struct DeviceSlot {
-  std::once_flag once;
-  cudaError_t status = cudaSuccess;
-  double* base = nullptr;
+  std::mutex mu;
+  double* base = nullptr;  // set once a lookup has succeeded
 };
 DeviceSlot g_slots[kMaxDevices];
 
-// Device address of the scratch array on the current device `dev`.
+// Device address of the scratch array on the current device `dev`. Only a
+// successful lookup is kept; after a failure the next call looks again.
 cudaError_t scratch_on(int dev, double** out) {
   DeviceSlot& s = g_slots[dev];
-  std::call_once(s.once, [&s]() {
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (!s.base) {
     void* p = nullptr;
-    s.status = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      *out = nullptr;
+      return e != cudaSuccess ? e : cudaErrorInvalidSymbol;
+    }
     s.base = static_cast<double*>(p);
-  });
+  }
   *out = s.base;
-  return s.status;
+  return cudaSuccess;
 }
 
 int max_coresident(int block, int dev) {
@@ -163,7 +179,10 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
   }
   const int cap = max_coresident(block, device);
   if (cap > 0 && grid > cap) grid = cap;
-  if (grid > kNoallocMaxBlocks) grid = kNoallocMaxBlocks;
+  if (grid > kNoallocMaxBlocks) {  // excluded by the static_asserts above
+    eaf::set_error_text("eaf_cg_solve_f64_noalloc: launch shape exceeds the static scratch");
+    return EAF_EINVAL;
+  }
 
   eaf::HaloInputs in = {aW, aE, aS, aN, aB, aT, aP, Su, phi};
   e = eaf::launch_pack_f64(d, in, s, st);

@@ -10,7 +10,7 @@ struct TunedWidth {
 };
 
 // Lane width (blocks of 512 threads) of batched and served solves.
-static const TunedWidth kTunedWidths[] = {
+static constexpr TunedWidth kTunedWidths[] = {
     {12, 24, 16, 1},
     {18, 36, 24, 4},
     {35, 70, 50, 24},
@@ -30,13 +30,21 @@ struct TunedLaunch {
 };
 
 // (block, grid) of the single-system persistent solver.
-static const TunedLaunch kTunedLaunches[] = {
+static constexpr TunedLaunch kTunedLaunches[] = {
     {12, 24, 16, 256, 8},
     {18, 36, 24, 256, 32},
     {35, 70, 50, 256, 148},
     {60, 120, 84, 512, 148},
     {120, 240, 168, 1024, 148},
 };
+
+// Largest tuned grid among meshes of at most `max_cells` cells (0 if none).
+constexpr int max_tuned_grid_up_to(long long max_cells) {
+  int g = 0;
+  for (const TunedLaunch& t : kTunedLaunches)
+    if ((long long)t.nr * t.nth * t.nz <= max_cells && t.grid > g) g = t.grid;
+  return g;
+}
 
 inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid) {
   for (const TunedLaunch& t : kTunedLaunches)

@@ -94,21 +94,40 @@ def _gpu_solve(arrays, phi, max_iter, tol):
     from . import CGSolver
     nr, nth, nz = phi.shape[2] - 4, phi.shape[1] - 4, phi.shape[0] - 4
     with CGSolver(nr, nth, nz) as cg:
-        res, nit, _ = cg.solve(arrays, phi, max_iter, tol)
-    return res, nit
+        return cg.solve(arrays, phi, max_iter, tol)
+
+
+class MultirankError(_lib.EafError):
+    """The root's gather, solve or scatter preparation failed; raised on
+    every rank of the collective, with the root's status and message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(status, "cg_3d_multirank (root): " + message)
 
 
 def cg_3d_multirank(local_arrays, phi_local: np.ndarray, nr: int, nth: int, nz: int,
                     max_iter: int, tol: float, group=None, root: int = 0,
-                    grid: tuple | None = None, coords: tuple | None = None, solve=None):
+                    grid: tuple | None = None, coords: tuple | None = None, solve=None,
+                    return_status: bool = False):
     """Collective over `group`: every rank passes its local (aW, aE, aS, aN,
     aB, aT, aP, Su) and phi (numpy, shape (kloc+4, jloc+4, iloc+4)); phi is
     updated in place (interior and in-domain halos). Returns (residual,
-    n_iter) on every rank. `solve(arrays, phi, max_iter, tol)` replaces the
-    root's GPU solve (default: the single-GPU CG on the current device)."""
+    n_iter) on every rank, or (residual, n_iter, status) with
+    `return_status`. `root` is a rank of `group`.
+
+    `solve(arrays, phi, max_iter, tol)` replaces the root's GPU solve
+    (default: the single-GPU CG on the current device) and returns
+    (residual, n_iter) or (residual, n_iter, status). A non-finite result is
+    not an error, as in the reference (src/mod_pressure_3d.f90:322): every
+    rank gets the NaN residual and status EAF_ENONFINITE. If anything on the
+    root fails (placing the blocks, the solve raising, e.g. EAF_ETIMEOUT or
+    EAF_ECUDA, or extracting them), every rank still completes the same
+    collectives and then raises MultirankError; phi is left as it was."""
     import torch.distributed as dist
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
+    # torch takes src/dst of the object collectives as global ranks
+    groot = root if group is None else dist.get_global_rank(group, root)
     grid = tuple(grid) if grid is not None else process_grid(world, nr, nth, nz)
     coords = tuple(coords) if coords is not None else rank_coords(rank, grid)
     loc, start = block(nr, nth, nz, grid, coords)
@@ -119,20 +138,34 @@ def cg_3d_multirank(local_arrays, phi_local: np.ndarray, nr: int, nth: int, nz: 
     payload = (coords, loc, start, [pack(a, grid, coords, loc)
                                     for a in list(local_arrays) + [phi_local]])
     gathered = [None] * world if rank == root else None
-    dist.gather_object(payload, gathered, dst=root, group=group)
+    dist.gather_object(payload, gathered, dst=groot, group=group)
     outs = None
+    # (residual, n_iter, status, error message or None)
     result = [None]
     if rank == root:
-        hshape = (nz + 4, nth + 4, nr + 4)
-        G = [np.zeros(hshape) for _ in range(9)]
-        for (c, l, s, bufs) in gathered:
-            for a, b in zip(G, bufs):
-                place(a, nr, nth, nz, grid, c, l, s, b)
-        res, nit = (solve or _gpu_solve)(G[:8], G[8], max_iter, tol)
-        outs = [extract(G[8], nr, nth, nz, l, s) for (_, l, s, _) in gathered]
-        result = [(float(res), int(nit))]
+        try:
+            hshape = (nz + 4, nth + 4, nr + 4)
+            G = [np.zeros(hshape) for _ in range(9)]
+            for (c, l, s, bufs) in gathered:
+                for a, b in zip(G, bufs):
+                    place(a, nr, nth, nz, grid, c, l, s, b)
+            out = (solve or _gpu_solve)(G[:8], G[8], max_iter, tol)
+            res, nit = float(out[0]), int(out[1])
+            st = int(out[2]) if len(out) > 2 else (
+                _lib.EAF_OK if np.isfinite(res) else _lib.EAF_ENONFINITE)
+            if st not in (_lib.EAF_OK, _lib.EAF_ENONFINITE):
+                raise _lib.EafError(st, "solve")
+            outs = [extract(G[8], nr, nth, nz, l, s) for (_, l, s, _) in gathered]
+            result = [(res, nit, st, None)]
+        except Exception as exc:  # reported to every rank below
+            outs = [None] * world
+            status = exc.status if isinstance(exc, _lib.EafError) else _lib.EAF_EINVAL
+            result = [(float("nan"), 0, int(status), f"{type(exc).__name__}: {exc}")]
     recv = [None]
-    dist.scatter_object_list(recv, outs, src=root, group=group)
+    dist.scatter_object_list(recv, outs, src=groot, group=group)
+    dist.broadcast_object_list(result, src=groot, group=group)
+    res, nit, st, err = result[0]
+    if err is not None:
+        raise MultirankError(st, err)
     unpack(phi_local, nr, nz, loc, start, recv[0])
-    dist.broadcast_object_list(result, src=root, group=group)
-    return result[0]
+    return (res, nit, st) if return_status else (res, nit)

@@ -15,7 +15,10 @@ Two oracle forms are used:
   the test therefore asserts the spread such implementations show:
   both residuals below tol, iteration counts within 5 % (at least 2; the
   serial and 8-thread oracles differ by 2.5 % at 60x120x84) and
-  solution relative-L2 difference <= 2e-8.
+  solution relative-L2 difference <= 2e-8. The reference's own operating
+  regime (50 iterations per call, src/mod_config_3d.f90:41) and the
+  production mesh to tol are held to tighter bars against the serial oracle
+  in tests/test_gpu_parity_serial.py.
 """
 import ctypes
 
@@ -112,20 +115,6 @@ def test_mesh_beyond_l2_fixed_iterations_bitwise(launch):
     res, nit, st, plan, _ = assert_bitwise(s, g.zeros_phi(100, 100, 80),
                                            max_iter=40, tol=0.0, launch=launch)
     assert nit == 40 and plan == (148, launch[0])
-
-
-def test_production_mesh_to_tol_vs_sequential_oracle():
-    """60x120x84 to 1e-8 against the threaded sequential-association oracle."""
-    import oracle
-    g = gen()
-    s = g.make_system(*g.PRODUCTION, seed=0)
-    phi_g = g.zeros_phi(60, 120, 84)
-    res_g, nit_g, st, _, _ = gpu_solve(s, phi_g)
-    phi_o = g.zeros_phi(60, 120, 84)
-    res_o, nit_o = oracle.cg(s, phi_o, 200000, TOL, nthreads=max(1, oracle.max_threads()))
-    assert st == 0 and res_g < TOL and res_o < TOL
-    assert abs(nit_g - nit_o) <= max(2, SEQ_ITER_FRAC * nit_o), (nit_g, nit_o)
-    assert rel_l2(phi_g, phi_o) <= SEQ_SOL_RTOL
 
 
 def test_warm_start_with_halo_values_bitwise():

@@ -175,3 +175,101 @@ def test_gloo_ranks_match_serial_solve(tmp_path, world, dims):
     run_ranks(world, dims, tmp_path)
     check_against_single(world, dims, tmp_path,
                          lambda s, phi: oracle.cg(s, phi, 5000, 1e-8))
+
+
+def _raising_solve(arrays, phi, max_iter, tol):
+    raise pkg().EafError(pkg()._lib.EAF_ETIMEOUT, "solve")
+
+
+def _failure_worker(rank, world, port, out_dir):
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        m = mr()
+        g = gen()
+        dims = (12, 24, 16)
+        s = g.make_system(*dims, nsph=4, seed=3)
+        grid = m.process_grid(world, *dims)
+        c = m.rank_coords(rank, grid)
+        loc, start = m.block(*dims, grid, c)
+        arrays = [local_from_global(a, *dims, loc, start) for a in s.arrays()]
+        phi = local_from_global(g.zeros_phi(*dims), *dims, loc, start)
+        before = phi.copy()
+        outcome = "returned"
+        try:
+            m.cg_3d_multirank(arrays, phi, *dims, 100, 1e-8, solve=_raising_solve)
+        except m.MultirankError as exc:
+            outcome = f"raised {exc.status}"
+        # the collective stays usable after the failure
+        dist.barrier()
+        np.save(os.path.join(out_dir, f"unchanged{rank}.npy"),
+                np.array([np.array_equal(phi, before)]))
+        with open(os.path.join(out_dir, f"outcome{rank}.txt"), "w") as f:
+            f.write(outcome)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_root_solve_failure_raises_on_every_rank(tmp_path):
+    """The root's solve raises (as a timed-out or failed GPU solve does):
+    every rank completes the collectives and raises MultirankError with the
+    root's status, phi untouched, and the process group still works."""
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_failure_worker, args=(world, _free_port(), str(tmp_path)),
+                       nprocs=world, join=True, start_method="spawn")
+    st = pkg()._lib.EAF_ETIMEOUT
+    for rank in range(world):
+        assert open(os.path.join(tmp_path, f"outcome{rank}.txt")).read() == f"raised {st}"
+        assert bool(np.load(os.path.join(tmp_path, f"unchanged{rank}.npy"))[0])
+
+
+def _subgroup_worker(rank, world, port, out_dir):
+    """Ranks 1 and 2 of 3 form the group; its rank 0 (global rank 1) is the
+    root."""
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        sub = dist.new_group([1, 2])
+        if rank in (1, 2):
+            m = mr()
+            g = gen()
+            dims = (12, 24, 16)
+            s = g.make_system(*dims, nsph=4, seed=3)
+            phi_g = np.random.default_rng(2).normal(0, 1e-4, size=g.halo_shape(*dims))
+            grank = dist.get_rank(sub)
+            grid = m.process_grid(2, *dims)
+            c = m.rank_coords(grank, grid)
+            loc, start = m.block(*dims, grid, c)
+            arrays = [local_from_global(a, *dims, loc, start) for a in s.arrays()]
+            phi = local_from_global(phi_g, *dims, loc, start)
+            res, nit = m.cg_3d_multirank(arrays, phi, *dims, 5000, 1e-8, group=sub,
+                                         root=0, solve=_oracle_solve)
+            np.save(os.path.join(out_dir, f"phi{grank}.npy"), phi)
+            np.save(os.path.join(out_dir, f"res{grank}.npy"), np.array([res, nit]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_subgroup_root_is_mapped_to_its_global_rank(tmp_path):
+    import oracle
+    import torch.multiprocessing as mp
+    mp.start_processes(_subgroup_worker, args=(3, _free_port(), str(tmp_path)),
+                       nprocs=3, join=True, start_method="spawn")
+    check_against_single(2, (12, 24, 16), tmp_path,
+                         lambda s, phi: oracle.cg(s, phi, 5000, 1e-8))

@@ -11,6 +11,9 @@ warm-started re-solve that reuses the array left by the first call) and
 compares each result with the handle-based eaf_cg_solve_f64_device on the
 same inputs. Both run the same kernels with the same launch shape, so the
 tolerance is exact equality: iteration count, residual and every phi value.
+Besides the two tuned meshes, two meshes outside the tuned table run the
+fallback launch rules (one 1024-thread block up to 8192 cells, else one
+512-thread block per 2048 cells), which this entry restates.
 The file is named to be collected last and also passes on its own.
 """
 import ctypes
@@ -33,8 +36,10 @@ def _noalloc(lib, s, dev_arrays, phi_dev, max_iter=100000, tol=1e-8):
     return st, res.value, nit.value
 
 
-@pytest.mark.parametrize("dims", [(12, 24, 16, 8), (18, 36, 24, 8)])
-def test_noalloc_matches_handle_entry_on_two_calls(dims):
+@pytest.mark.parametrize("dims,launch", [((12, 24, 16, 8), None), ((18, 36, 24, 8), None),
+                                         ((10, 20, 12, 4), (1, 1024)),
+                                         ((20, 40, 30, 8), (12, 512))])
+def test_noalloc_matches_handle_entry_on_two_calls(dims, launch):
     torch = pytest.importorskip("torch")
     eaf = pkg()
     g = gen()
@@ -55,6 +60,8 @@ def test_noalloc_matches_handle_entry_on_two_calls(dims):
             assert res_a < 1e-8
             assert (nit_a, res_a) == (nit_b, res_b)
             assert torch.equal(phi_a, phi_b)
+            if launch is not None:
+                assert cg.last_launch() == launch
 
 
 def test_noalloc_refuses_meshes_above_its_limit():
