@@ -254,7 +254,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     solver = eaf.CGSolver(nr, nth, nz, device=dev)
     solver.set_form(CG_FORMS[args.cg_form])
-    block, grid = solver.launch()
+    if args.cluster is not None:
+        solver.set_cluster(args.cluster)
 
     def one(k, resident=True, host_arrays=None, phi_h=None):
         if resident:
@@ -284,6 +285,7 @@ def run_ours(args, rank, world, local_rank):
         kern_ms += t["kernel_ms"]
     torch.cuda.synchronize()
     clk = clocks.stop()
+    plan = solver.last_launch()
     if dist is not None:
         dist.barrier()
 
@@ -338,7 +340,8 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": "pressure-CG 60x120x84 FP64 warm-started re-solves",
                    "mesh": [nr, nth, nz], "cells": n, "spheres": nsph, "tol": TOL,
                    "iterations_per_solve": iters,
-                   "launch": {"grid": grid, "block": block},
+                   "launch": {"grid": plan[0], "block": plan[1],
+                              "cluster": plan[2] if len(plan) > 2 else 1},
                    "cg_form": args.cg_form,
                    "l2": "flushed between steps (256 MiB memset); within a solve "
                          "the ~39 MB symmetric working set is L2-resident",
@@ -350,7 +353,8 @@ def run_ours(args, rank, world, local_rank):
                      "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read+write of one bench "
                                        "launch (profiles/cg_f64_kernel_60x120x84.txt)",
-                     "kernel": "cg_f64_kernel (persistent, one launch per solve)",
+                     "kernel": ("cg_cluster_kernel" if len(plan) > 2 else "cg_f64_kernel")
+                               + " (persistent, one launch per solve)",
                      "algorithmic_bytes_per_cell_iter": BYTES_PER_CELL_ITER},
         "cpu_baseline": ({k: v for k, v in cpu.items() if k != "seconds"}
                          if cpu else None),
@@ -955,6 +959,8 @@ def run_fixed(args):
             cg.set_form(CG_FORMS[args.cg_form])
             if args.launch:
                 cg.set_launch(*args.launch)
+            if args.cluster is not None:
+                cg.set_cluster(args.cluster)
             for _ in range(args.repeat):
                 phi.zero_()
                 torch.cuda.synchronize()
@@ -991,6 +997,9 @@ def main(argv=None):
     ap.add_argument("--cg-form", choices=sorted(CG_FORMS), default=DEFAULT_CG_FORM,
                     help="FP64 CG recurrences: the reference's (two all-reduces per "
                          "iteration) or the single-reduction rearrangement")
+    ap.add_argument("--cluster", type=int, default=None,
+                    help="blocks per thread-block cluster of the FP64 CG (1 = none, "
+                         "0 = the tuned choice; default: the tuned choice)")
     ap.add_argument("--mixed-outer", type=int, default=30)
     ap.add_argument("--mixed-inner", type=int, default=3000)
     ap.add_argument("--rates", default="5,20,50,200")

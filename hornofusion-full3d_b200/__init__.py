@@ -257,10 +257,30 @@ class CGSolver:
         return b.value, g.value
 
     def last_launch(self) -> tuple:
-        """(grid, block) of the last solve: the oracle plan of its dots."""
-        b, g = ctypes.c_int(), ctypes.c_int()
+        """The oracle plan of the last solve's dots: (grid, block), or
+        (grid, block, cluster) when it ran on a grid of thread-block
+        clusters."""
+        b, g, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(self._lib.eaf_cg_last_launch(self._h, ctypes.byref(b), ctypes.byref(g)))
-        return g.value, b.value
+        check(self._lib.eaf_cg_last_cluster(self._h, ctypes.byref(c)))
+        return (g.value, b.value) if c.value <= 1 else (g.value, b.value, c.value)
+
+    def set_cluster(self, cluster: int = 0) -> None:
+        """Blocks per thread-block cluster of the plain FP64 solve: 2..16,
+        1 for none, 0 for the tuned choice of the mesh."""
+        check(self._lib.eaf_cg_set_cluster(self._h, int(cluster)), "set_cluster")
+
+    def set_resident(self, resident: bool = True) -> None:
+        """One-cluster launches of a mesh that fits keep the system in the
+        cluster's shared memory (default) or run the global-memory cluster
+        kernel; both give the same bits."""
+        check(self._lib.eaf_cg_set_resident(self._h, int(bool(resident))), "set_resident")
+
+    def cluster(self) -> int:
+        """Blocks per cluster the next plain FP64 solve runs with."""
+        c = ctypes.c_int()
+        check(self._lib.eaf_cg_get_cluster(self._h, ctypes.byref(c)), "get_cluster")
+        return c.value
 
     FORM_REFERENCE = 0
     FORM_ONE_REDUCTION = 1

@@ -7,7 +7,9 @@ counts (tol 0) and CUDA-event device times from the library:
 
 * single-system solver (eaf_cg_*): the time per iteration of the persistent
   kernel for block sizes 256/512/1024 and grid sizes from one block up to
-  the co-resident maximum; the fastest (block, grid) is kept;
+  the co-resident maximum, and, on meshes that fit one cluster's shared
+  memory, the cluster-resident kernel on one cluster of 4, 8 or 16 blocks of
+  128 to 1024 threads; the fastest (block, grid, cluster) is kept;
 * batched/served solver (eaf_batch_*): the time per iteration t(w) of one
   system on a lane of w blocks of 512 threads. A batch is limited by the
   block-time its systems take (t(w) * w per iteration) and by its longest
@@ -34,6 +36,7 @@ sys.path.insert(0, ROOT)
 MESHES = [(12, 24, 16, 8), (18, 36, 24, 8), (35, 70, 50, 16), (60, 120, 84, 24),
           (120, 240, 168, 64)]
 LATENCY_SLACK = 2.5
+RESIDENT_MAX_CELLS = 35000
 
 
 def select(log):
@@ -48,7 +51,7 @@ def select(log):
         sm = [m for m in log if tuple(m["mesh"]) == d and m["solver"] == "single"]
         if sm:
             b = min(sm, key=lambda m: (m["us_per_iter"], m["block"], m["grid"]))
-            single.append((d, b["block"], b["grid"], b["us_per_iter"]))
+            single.append((d, b["block"], b["grid"], b.get("cluster", 1), b["us_per_iter"]))
         lm = [m for m in log if tuple(m["mesh"]) == d and m["solver"] == "lane"]
         if lm:
             tmin = min(m["us_per_iter"] for m in lm)
@@ -58,9 +61,10 @@ def select(log):
     return single, lanes
 
 
-def time_single(eaf, dev_arrays, phi, dims, block, grid, iters):
+def time_single(eaf, dev_arrays, phi, dims, block, grid, iters, cluster=1):
     with eaf.CGSolver(*dims) as cg:
         cg.set_launch(block, grid)
+        cg.set_cluster(cluster)
         best = float("inf")
         for _ in range(2):
             phi.zero_()
@@ -94,8 +98,8 @@ def main(argv=None) -> int:
         with open(args.from_json) as f:
             res = json.load(f)
         single, lanes = select(res["measurements"])
-        res["single"] = [{"mesh": list(d), "block": b, "grid": gr, "us_per_iter": u}
-                         for d, b, gr, u in single]
+        res["single"] = [{"mesh": list(d), "block": b, "grid": gr, "cluster": c,
+                          "us_per_iter": u} for d, b, gr, c, u in single]
         res["lanes"] = [{"mesh": list(d), "width": w, "us_per_iter": u}
                         for d, w, u in lanes]
         res["lane_rule"] = f"least t(w)*w among t(w) <= {LATENCY_SLACK} x min t"
@@ -128,6 +132,13 @@ def main(argv=None) -> int:
             us, used = time_single(eaf, dev, phi, dims, block, grid, args.iters)
             log.append({"mesh": dims, "solver": "single", "block": block, "grid": used[0],
                         "us_per_iter": round(us, 3)})
+        if n <= RESIDENT_MAX_CELLS:  # one cluster holding the system on chip
+            for c in (4, 8, 16):
+                for block in (128, 256, 288, 512, 1024):
+                    us, used = time_single(eaf, dev, phi, dims, block, c, args.iters, c)
+                    if len(used) == 3 and used[0] == c:
+                        log.append({"mesh": dims, "solver": "single", "block": block,
+                                    "grid": c, "cluster": c, "us_per_iter": round(us, 3)})
         if n <= 1_000_000:  # batched/served meshes
             widths = [w for w in (1, 2, 4, 8, 16, 24, 32, 48, 64, 96, 128)
                       if w * 512 <= max(2 * n, 512)]
@@ -140,8 +151,8 @@ def main(argv=None) -> int:
     single, lanes = select(log)
     result = {"gpu": torch.cuda.get_device_name(0), "iters": args.iters,
               "lane_rule": f"least t(w)*w among t(w) <= {LATENCY_SLACK} x min t",
-              "single": [{"mesh": d, "block": b, "grid": gr, "us_per_iter": round(u, 3)}
-                         for d, b, gr, u in single],
+              "single": [{"mesh": d, "block": b, "grid": gr, "cluster": c,
+                          "us_per_iter": round(u, 3)} for d, b, gr, c, u in single],
               "lanes": [{"mesh": d, "width": w, "us_per_iter": round(u, 3)}
                         for d, w, u in lanes],
               "measurements": log}
@@ -159,7 +170,8 @@ def main(argv=None) -> int:
 
 def write_header(single, lanes, path):
     rows_l = "\n".join(f"    {{{d[0]}, {d[1]}, {d[2]}, {w}}}," for d, w, _ in lanes)
-    rows_s = "\n".join(f"    {{{d[0]}, {d[1]}, {d[2]}, {b}, {gr}}}," for d, b, gr, _ in single)
+    rows_s = "\n".join(f"    {{{d[0]}, {d[1]}, {d[2]}, {b}, {gr}, {c}}},"
+                       for d, b, gr, c, _ in single)
     text = f"""// Launch shapes measured on B200 by hornofusion-full3d_b200/autotune.py
 // (tune_table.json beside it holds every measurement). Meshes that are not
 // in a table fall back to the rules below.
@@ -185,27 +197,33 @@ inline int tuned_lane_width(int nr, int nth, int nz) {{
 }}
 
 struct TunedLaunch {{
-  int nr, nth, nz, block, grid;
+  int nr, nth, nz, block, grid, cluster;
 }};
 
-// (block, grid) of the single-system persistent solver.
+// (block, grid, blocks per cluster; 1 = no clusters) of the single-system
+// persistent solver.
 static constexpr TunedLaunch kTunedLaunches[] = {{
 {rows_s}
 }};
 
-// Largest tuned grid among meshes of at most `max_cells` cells (0 if none).
+// Most blocks a tuned launch of a mesh of at most `max_cells` cells can run
+// (a grid is raised to one whole cluster at least); 0 if there is none.
 constexpr int max_tuned_grid_up_to(long long max_cells) {{
   int g = 0;
-  for (const TunedLaunch& t : kTunedLaunches)
-    if ((long long)t.nr * t.nth * t.nz <= max_cells && t.grid > g) g = t.grid;
+  for (const TunedLaunch& t : kTunedLaunches) {{
+    const int blocks = t.grid > t.cluster ? t.grid : t.cluster;
+    if ((long long)t.nr * t.nth * t.nz <= max_cells && blocks > g) g = blocks;
+  }}
   return g;
 }}
 
-inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid) {{
+inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid,
+                                int* cluster = nullptr) {{
   for (const TunedLaunch& t : kTunedLaunches)
     if (t.nr == nr && t.nth == nth && t.nz == nz) {{
       *block = t.block;
       *grid = t.grid;
+      if (cluster) *cluster = t.cluster;
       return true;
     }}
   return false;

@@ -32,6 +32,7 @@ UNITS = {
     "api.cu": [],
     "api_pressure.cu": [],
     "cg_f64.cu": ["-fmad=false"],
+    "cg_dsm.cu": ["-fmad=false"],
     "cg_mixed.cu": [],
     "batch.cu": [],
     "noalloc.cu": ["-fmad=false"],

@@ -10,6 +10,7 @@
 #include <new>
 
 #include "cg_kernels.h"
+#include "cluster_red.cuh"
 #include "eafcg.h"
 #include "eafcg_internal.h"
 #include "handle.h"
@@ -26,6 +27,9 @@ namespace {
 
 constexpr int kPartSlots = 8;
 constexpr int kDefaultBlock = 512;
+// Doubles of a handle's partial table (also the slot table of the cluster
+// all-reduce).
+inline size_t kPartTableDoubles(const eaf_cg* h) { return (size_t)kPartSlots * h->sms * 8; }
 constexpr uint64_t kDefaultTimeoutNs = 2000ull * 1000ull * 1000ull;
 
 }  // namespace
@@ -92,38 +96,91 @@ static int max_coresident(const void* kernel, int block, int sms) {
   return per_sm * sms;
 }
 
+namespace eaf {
+
 // Launch shape for a persistent kernel over n cells: an explicit
 // eaf_cg_set_launch shape, else the tuned shape of this mesh (FP64 solver),
 // else one 1024-thread block up to 8192 cells or one 512-thread block per
 // 2048 cells; capped by co-residency of the kernel (variant) that runs
-// blocks of that size.
-static void pick_launch(const eaf_cg* h, bool f64, int* grid, int* block) {
-  auto kernel_for = [f64, h](int b) {
-    if (!f64) return eaf::cg_mixed_kernel_ptr();
-    return h->form == EAF_CG_FORM_ONE_REDUCTION ? eaf::cg1_f64_kernel_ptr(b)
-                                                : eaf::cg_f64_kernel_ptr(b, h->d.n);
+// blocks of that size. The reference-form FP64 solver may run on a grid of
+// thread-block clusters (eaf_cg_set_cluster, else the tuned cluster size):
+// the grid is then a whole number of clusters, at most as many as can be
+// resident; a cluster size the device cannot launch falls back to none.
+SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int req_grid,
+                           int req_cluster, int form, bool f64) {
+  const long long n = (long long)nr * nth * nz;
+  auto kernel_for = [f64, form, n](int b) {
+    if (!f64) return cg_mixed_kernel_ptr();
+    return form == EAF_CG_FORM_ONE_REDUCTION ? cg1_f64_kernel_ptr(b) : cg_f64_kernel_ptr(b, n);
   };
-  int b = h->block > 0 ? h->block : kDefaultBlock;
+  int b = req_block > 0 ? req_block : kDefaultBlock;
   int g;
-  int tb = 0, tg = 0;
-  if (h->block == 0 && h->grid == 0 && f64 &&
-      eaf::tuned_single_launch(h->nr, h->nth, h->nz, &tb, &tg)) {
+  int tb = 0, tg = 0, tc = 1;
+  const bool automatic = req_block == 0 && req_grid == 0;
+  if (automatic && f64 && tuned_single_launch(nr, nth, nz, &tb, &tg, &tc)) {
     b = tb;
     g = tg;
-  } else if (h->grid > 0) {
-    g = h->grid;
-  } else if (h->d.n <= 8192) {
-    b = h->block > 0 ? h->block : 1024;
+  } else if (req_grid > 0) {
+    g = req_grid;
+  } else if (n <= 8192) {
+    b = req_block > 0 ? req_block : 1024;
     g = 1;
   } else {
-    long long want = ((long long)h->d.n + (long long)b * 4 - 1) / ((long long)b * 4);
+    long long want = (n + (long long)b * 4 - 1) / ((long long)b * 4);
     g = (int)(want < 1 ? 1 : want);
   }
-  const int cap = max_coresident(kernel_for(b), b, h->sms);
-  if (cap > 0 && g > cap) g = cap;
-  if (g > h->sms * 8) g = h->sms * 8;
-  *grid = g;
-  *block = b;
+  int c = 1;
+  if (f64 && form == EAF_CG_FORM_REFERENCE) {
+    c = req_cluster > 0 ? req_cluster : (automatic ? tc : 1);
+    if (c > 1) {
+      const int active = max_active_clusters(b, n, c);
+      if (active < 1) {
+        c = 1;
+      } else {
+        if (g < c) g = c;
+        g -= g % c;
+        int ncl = g / c;
+        if (ncl > active) ncl = active;
+        if (ncl > kMaxClusters) ncl = kMaxClusters;
+        g = ncl * c;
+      }
+    }
+  }
+  if (c == 1) {
+    const int cap = max_coresident(kernel_for(b), b, sms);
+    if (cap > 0 && g > cap) g = cap;
+    if (g > sms * 8) g = sms * 8;
+  }
+  SolverLaunch L;
+  L.grid = g;
+  L.block = b;
+  L.cluster = c;
+  return L;
+}
+
+bool runs_resident(const SolverLaunch& L, long long n, bool allowed) {
+  return allowed && L.cluster > 1 && L.grid == L.cluster && n <= dsm_max_cells(L.cluster);
+}
+
+cudaError_t launch_f64_solver(const SolverLaunch& L, bool resident, const MeshDims& d,
+                              const SysF64& s, const GroupWs& ws, size_t slot_doubles,
+                              int max_iter, double tol, uint64_t timeout_ns, cudaStream_t st) {
+  if (runs_resident(L, d.n, resident))
+    return launch_cg_f64_dsm(d, s, ws, max_iter, tol, L.block, L.cluster, st);
+  if (L.cluster > 1)
+    return launch_cg_f64_cluster(d, s, ws, ws.part, slot_doubles, max_iter, tol, timeout_ns,
+                                 L.grid, L.block, L.cluster, st);
+  return launch_cg_f64(d, s, ws, max_iter, tol, timeout_ns, L.grid, L.block, st);
+}
+
+}  // namespace eaf
+
+static void pick_launch(const eaf_cg* h, bool f64, int* grid, int* block, int* cluster) {
+  const eaf::SolverLaunch L = eaf::choose_launch(h->nr, h->nth, h->nz, h->sms, h->block,
+                                                 h->grid, h->cluster, h->form, f64);
+  *grid = L.grid;
+  *block = L.block;
+  *cluster = L.cluster;
 }
 
 extern "C" {
@@ -172,6 +229,7 @@ int eaf_cg_create_mesh(eaf_cg_t* out, int nr, int nth, int nz, int is_parallel,
   h->d = eaf::make_dims(nr, nth, nz);
   h->nh = (size_t)nh;
   h->timeout_ns = kDefaultTimeoutNs;
+  h->resident = 1;
   int rc = EAF_OK;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** p, size_t bytes) {
@@ -190,7 +248,7 @@ int eaf_cg_create_mesh(eaf_cg_t* out, int nr, int nth, int nz, int is_parallel,
     e = cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
   h->sms = dev_sms > 0 ? dev_sms : 148;
 
-  alloc((void**)&h->ws.part, sizeof(double) * kPartSlots * h->sms * 8);
+  alloc((void**)&h->ws.part, sizeof(double) * kPartTableDoubles(h));
   alloc((void**)&h->ws.counter, sizeof(unsigned long long));
   alloc((void**)&h->ws.err, sizeof(int));
   alloc((void**)&h->ws.result, sizeof(SolveResult));
@@ -233,7 +291,8 @@ int eaf_cg_set_launch(eaf_cg_t h, int block_threads, int grid_blocks) {
 int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks) {
   if (!h || !block_threads || !grid_blocks) return EAF_EINVAL;
   eaf::DeviceGuard guard(h->device);
-  pick_launch(h, true, grid_blocks, block_threads);
+  int cluster = 1;
+  pick_launch(h, true, grid_blocks, block_threads, &cluster);
   return EAF_OK;
 }
 
@@ -241,6 +300,32 @@ int eaf_cg_last_launch(eaf_cg_t h, int* block_threads, int* grid_blocks) {
   if (!h || !block_threads || !grid_blocks) return EAF_EINVAL;
   *block_threads = h->last_block;
   *grid_blocks = h->last_grid;
+  return EAF_OK;
+}
+
+int eaf_cg_set_cluster(eaf_cg_t h, int cluster_blocks) {
+  if (!h || cluster_blocks < 0 || cluster_blocks > eaf::kMaxClusterSize) return EAF_EINVAL;
+  h->cluster = cluster_blocks;
+  return EAF_OK;
+}
+
+int eaf_cg_get_cluster(eaf_cg_t h, int* cluster_blocks) {
+  if (!h || !cluster_blocks) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  int grid = 0, block = 0;
+  pick_launch(h, true, &grid, &block, cluster_blocks);
+  return EAF_OK;
+}
+
+int eaf_cg_set_resident(eaf_cg_t h, int resident) {
+  if (!h || (resident != 0 && resident != 1)) return EAF_EINVAL;
+  h->resident = resident;
+  return EAF_OK;
+}
+
+int eaf_cg_last_cluster(eaf_cg_t h, int* cluster_blocks) {
+  if (!h || !cluster_blocks) return EAF_EINVAL;
+  *cluster_blocks = h->last_cluster > 0 ? h->last_cluster : 1;
   return EAF_OK;
 }
 
@@ -335,27 +420,30 @@ static int ensure_f32(eaf_cg* h) {
 int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts& o) {
   EAF_CUDA(cudaEventRecord(h->ev[1], h->st));
   EAF_CUDA(eaf::launch_pack_f64(h->d, in, h->s, h->st));
-  int grid, block;
+  int grid, block, cluster = 1;
   if (o.mixed) {
     int rc = ensure_f32(h);
     if (rc != EAF_OK) return rc;
-    pick_launch(h, false, &grid, &block);
+    pick_launch(h, false, &grid, &block, &cluster);
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     EAF_CUDA(eaf::launch_cg_mixed(h->d, h->s, h->f, h->ws, o.max_outer, o.max_iter,
                                   o.tol, o.inner_tol, h->timeout_ns, grid, block,
                                   h->st));
   } else {
-    pick_launch(h, true, &grid, &block);
+    pick_launch(h, true, &grid, &block, &cluster);
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     if (h->form == EAF_CG_FORM_ONE_REDUCTION)
       EAF_CUDA(eaf::launch_cg1_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
                                    grid, block, h->st));
     else
-      EAF_CUDA(eaf::launch_cg_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
-                                  grid, block, h->st));
+      EAF_CUDA(eaf::launch_f64_solver(eaf::SolverLaunch{grid, block, cluster},
+                                      h->resident != 0, h->d, h->s, h->ws,
+                                      kPartTableDoubles(h), o.max_iter, o.tol,
+                                      h->timeout_ns, h->st));
   }
   h->last_grid = grid;
   h->last_block = block;
+  h->last_cluster = cluster;
   EAF_CUDA(cudaEventRecord(h->ev[3], h->st));
   EAF_CUDA(eaf::launch_unpack_f64(h->d, h->s.x, phi, h->st));
   EAF_CUDA(cudaEventRecord(h->ev[4], h->st));

@@ -31,6 +31,7 @@ int enqueue_tdma(eaf_cg* h, const HaloInputs& in, double* phi, int n_sweep) {
   }
   h->last_grid = eaf::tdma_grid(h->nr, h->nth, h->nz);
   h->last_block = 64;
+  h->last_cluster = 1;
   EAF_CUDA(cudaEventRecord(h->ev[1], h->st));
   EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
   if (n_sweep > 0) {
@@ -73,6 +74,7 @@ int run_residual(eaf_cg* h, const HaloInputs& in, const double* phi, double* res
   residual_launch_shape(h, &grid, &block);
   h->last_grid = grid;
   h->last_block = block;
+  h->last_cluster = 1;
   EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
   EAF_CUDA(eaf::launch_residual_f64(in, phi, h->d, h->ws, h->timeout_ns, grid, block,
                                     h->st));

@@ -19,6 +19,7 @@
 #include <math.h>
 
 #include "cg_kernels.h"
+#include "cluster_red.cuh"
 #include "stencil.cuh"
 
 namespace eaf {
@@ -54,6 +55,19 @@ __device__ __forceinline__ void l2_prefetch_cells(const double* a, int lo, int h
                : "memory");
 }
 
+// The group all-reduce of a persistent solver, by the kind of group: a flat
+// group of co-resident blocks (one global stage over all blocks) or a grid
+// of thread-block clusters (shared-memory stage per cluster, global stage
+// among cluster leaders).
+template <int NV>
+__device__ __forceinline__ bool allsum(double (&v)[NV], Group& g, int slot) {
+  return group_allsum<NV>(v, g, slot);
+}
+template <int NV>
+__device__ __forceinline__ bool allsum(double (&v)[NV], ClusterGroup& g, int) {
+  return cluster_allsum<NV>(v, g);
+}
+
 struct CgArgs {
   MeshDims d;
   SysF64 s;
@@ -74,8 +88,8 @@ struct CgArgs {
 // phase. Kernels pick them by their register budget. PF: threads 0..7 of the
 // block prefetch the block's next round of every streamed array into L2
 // (one bulk prefetch per array), for meshes whose working set exceeds L2.
-template <bool SYM, int U, int UA, bool PF>
-__device__ void cg_body(const CgArgs& a, Group& g) {
+template <bool SYM, int U, int UA, bool PF, class G>
+__device__ void cg_body(const CgArgs& a, G& g) {
   const MeshDims& d = a.d;
   const SysF64& s = a.s;
   const Slice own = own_slice(d.n, g.nb, g.bid);
@@ -114,7 +128,7 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
       }
     }
   }
-  bool ok = group_allsum<3>(v3, g, 0);
+  bool ok = allsum<3>(v3, g, 0);
   const double bnorm = sqrt(v3[0]);
   double residual = 0.0;
   int n_iter = 0;
@@ -184,7 +198,7 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
           }
         }
       }
-      if (!(ok = group_allsum<1>(v1, g, 3))) break;
+      if (!(ok = allsum<1>(v1, g, 3))) break;
       const double pq = v1[0];
       if (fabs(pq) < kSmall) break;
       const double alpha = rz / pq;
@@ -222,7 +236,7 @@ __device__ void cg_body(const CgArgs& a, Group& g) {
           v2[1] = v2[1] + (live ? rn * zv : 0.0);
         }
       }
-      if (!(ok = group_allsum<2>(v2, g, 4))) break;
+      if (!(ok = allsum<2>(v2, g, 4))) break;
       residual = sqrt(v2[0]) / bnorm;
       n_iter = iter;
       if (residual < a.tol) break;
@@ -272,6 +286,31 @@ __global__ void __launch_bounds__(MAXB, 1) cg_f64_kernel(CgArgs a) {
     cg_body<true, U, UA, PF>(a, g);
   else
     cg_body<false, U, UA, PF>(a, g);
+}
+
+// The same solver on a grid of thread-block clusters (cluster_red.cuh): the
+// blocks, their slices and the per-cell arithmetic are those of
+// cg_f64_kernel; only the all-reduces (and with them the association of the
+// dot products) differ.
+template <int MAXB, int U, int UA, bool PF>
+__global__ void __launch_bounds__(MAXB, 1) cg_cluster_kernel(CgArgs a, double* slots) {
+  ClusterGroup g = make_cluster_group(slots, a.ws.err, a.timeout_ns);
+  // Every block of the cluster has started before any block addresses
+  // another's shared memory.
+  cluster_sync_all();
+  if (*a.s.asym == 0)
+    cg_body<true, U, UA, PF>(a, g);
+  else
+    cg_body<false, U, UA, PF>(a, g);
+  // No block leaves while another block of its cluster may still address
+  // its shared memory.
+  cluster_sync_all();
+}
+
+__global__ void fill_marker_kernel(double* p, int n) {
+  const double marker = __longlong_as_double((long long)kSlotMarker);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = marker;
 }
 
 // ---------------------------------------------------------------------------
@@ -499,9 +538,9 @@ __global__ void __launch_bounds__(kBatchBlock, 2) batch_f64_kernel(BatchF64Args 
     ca.tol = a.tol;
     ca.timeout_ns = a.timeout_ns;
     if (*bs.s.asym == 0)
-      cg_body<true, 2, 1, false>(ca, g);
+      cg_body<true, 2, 1, false, Group>(ca, g);
     else
-      cg_body<false, 2, 1, false>(ca, g);
+      cg_body<false, 2, 1, false, Group>(ca, g);
   }
 }
 
@@ -679,6 +718,88 @@ const void* cg1_f64_kernel_ptr(int block) {
   if (block <= 256) return (const void*)cg1_f64_kernel<256, 4>;
   if (block <= 512) return (const void*)cg1_f64_kernel<512, 2>;
   return (const void*)cg1_f64_kernel<1024, 1>;
+}
+
+const void* cg_cluster_kernel_ptr(int block, long long n) {
+  if (block <= 256) return (const void*)cg_cluster_kernel<256, 4, 4, false>;
+  if (block <= 512) return (const void*)cg_cluster_kernel<512, 4, 2, false>;
+  if (l2_prefetch_pays(n)) return (const void*)cg_cluster_kernel<1024, 2, 1, true>;
+  return (const void*)cg_cluster_kernel<1024, 2, 1, false>;
+}
+
+static cudaLaunchConfig_t cluster_config(int grid, int block, int cluster, cudaStream_t st,
+                                         cudaLaunchAttribute* attr, bool cooperative) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeCooperative;
+  attr[1].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = cooperative ? 2 : 1;
+  return cfg;
+}
+
+static cudaError_t allow_cluster_size(const void* k, int cluster) {
+  if (cluster <= 8) return cudaSuccess;
+  return cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+int max_active_clusters(int block, long long n, int cluster) {
+  if (cluster < 1 || cluster > kMaxClusterSize) return 0;
+  const void* k = cg_cluster_kernel_ptr(block, n);
+  if (allow_cluster_size(k, cluster) != cudaSuccess) return 0;
+  cudaLaunchAttribute attr[2];
+  cudaLaunchConfig_t cfg = cluster_config(cluster, block, cluster, nullptr, attr, false);
+  int count = 0;
+  if (cudaOccupancyMaxActiveClusters(&count, k, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return count;
+}
+
+cudaError_t launch_cg_f64_cluster(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                                  double* slots, size_t slot_doubles, int max_iter,
+                                  double tol, uint64_t timeout_ns, int grid, int block,
+                                  int cluster, cudaStream_t st) {
+  if (cluster < 2 || cluster > kMaxClusterSize || grid % cluster != 0 ||
+      grid / cluster > kMaxClusters || cluster_slot_doubles(grid / cluster) > slot_doubles)
+    return cudaErrorInvalidValue;
+  CgArgs a;
+  a.d = d;
+  a.s = s;
+  a.ws = ws;
+  a.max_iter = max_iter;
+  a.tol = tol;
+  a.timeout_ns = timeout_ns;
+  const void* k = cg_cluster_kernel_ptr(block, d.n);
+  cudaError_t e = allow_cluster_size(k, cluster);
+  if (e != cudaSuccess) return e;
+  (void)cudaGetLastError();  // report this launch's error, not an older one
+  const int nslots = (int)cluster_slot_doubles(grid / cluster);
+  fill_marker_kernel<<<(nslots + 255) / 256, 256, 0, st>>>(slots, nslots);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  void* args[] = {&a, &slots};
+  cudaLaunchAttribute attr[2];
+  cudaLaunchConfig_t cfg = cluster_config(grid, block, cluster, st, attr, true);
+  e = cudaLaunchKernelExC(&cfg, k, args);
+  if (e != cudaSuccess) {
+    // Without the cooperative attribute the launch is the same; every wait
+    // in the kernel is bounded, so blocks that were not co-scheduled end in
+    // EAF_ETIMEOUT rather than a hang.
+    (void)cudaGetLastError();
+    cfg = cluster_config(grid, block, cluster, st, attr, false);
+    e = cudaLaunchKernelExC(&cfg, k, args);
+  }
+  return e;
 }
 
 bool l2_prefetch_pays(long long n) { return (double)n * 128.0 > 96.0e6; }

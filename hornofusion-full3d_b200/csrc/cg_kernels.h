@@ -83,6 +83,45 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
 // same bits for one launch shape.
 bool l2_prefetch_pays(long long n);
 const void* cg_f64_kernel_ptr(int block, long long n);
+// The same solver on a grid of thread-block clusters of `cluster` blocks
+// (2..16; grid a multiple of it, at most 128 clusters): its all-reduces fold
+// through the leader block's shared memory in each cluster and a global
+// stage among the leaders only (cluster_red.cuh). `slots` holds at least
+// cluster_slot_doubles(grid / cluster) doubles (the handle's partial table
+// serves). Returns cudaErrorInvalidValue for a shape it cannot run.
+cudaError_t launch_cg_f64_cluster(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                                  double* slots, size_t slot_doubles, int max_iter,
+                                  double tol, uint64_t timeout_ns, int grid, int block,
+                                  int cluster, cudaStream_t st);
+// Clusters of `cluster` blocks of `block` threads that can be resident at
+// once (0 if the size cannot be launched).
+int max_active_clusters(int block, long long n, int cluster);
+// The same solve on ONE cluster of `cluster` blocks whose shared memory holds
+// the whole system for the whole solve (cg_dsm.cu); bit-identical to the
+// cluster kernel on the launch (cluster, block, cluster). Meshes of at most
+// dsm_max_cells(cluster) cells (about 35,000 at 16 blocks on B200).
+cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                              int max_iter, double tol, int block, int cluster,
+                              cudaStream_t st);
+int dsm_max_cells(int cluster);
+
+// Launch of a persistent single-system solver: blocks, threads per block,
+// blocks per thread-block cluster (1 = none).
+struct SolverLaunch {
+  int grid, block, cluster;
+};
+// The launch a handle with the requested shape (0 = automatic) uses on an
+// nr x nth x nz mesh (api.cu): the tuned shape, else the fallback rules,
+// with the cluster size and grid clamped to what the device can run.
+SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int req_grid,
+                           int req_cluster, int form, bool f64);
+// Whether the plain FP64 solve on launch L runs the cluster-resident kernel.
+bool runs_resident(const SolverLaunch& L, long long n, bool allowed);
+// Enqueues the plain FP64 solver (reference form) on launch L: the flat,
+// cluster or cluster-resident kernel; `slot_doubles` is the size of ws.part.
+cudaError_t launch_f64_solver(const SolverLaunch& L, bool resident, const MeshDims& d,
+                              const SysF64& s, const GroupWs& ws, size_t slot_doubles,
+                              int max_iter, double tol, uint64_t timeout_ns, cudaStream_t st);
 // Single-reduction (Chronopoulos-Gear) form of the same PCG: one group
 // all-reduce per iteration; uses s0/s1 and reuses r, z, q, p2 as the
 // double-buffered r and w = A M^-1 r.

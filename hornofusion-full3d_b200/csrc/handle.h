@@ -22,12 +22,14 @@ struct eaf_cg {
   eaf::GroupWs ws;
   eaf::SolveResult* res_h;  // pinned
   int block, grid;     // 0 = automatic
+  int cluster;         // blocks per thread-block cluster; 0 = automatic, 1 = none
+  int resident;        // one-cluster launches keep the system in shared memory
   int sms;
   uint64_t timeout_ns;
   cudaEvent_t ev[6];   // e2e0, solve0, kern0, kern1, solve1, e2e1
   double last_solve_ms, last_kernel_ms, last_e2e_ms;
   int last_sym, last_kernels;
-  int last_grid, last_block;
+  int last_grid, last_block, last_cluster;
   double* tdma_mbox;  // TDMA line hand-over slots (lazy)
   double* tdma_fac;  // TDMA line factors (lazy)
   double* pc_d;      // post-CG correction mirror: doubles (lazy)

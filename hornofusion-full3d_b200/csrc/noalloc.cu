@@ -24,8 +24,8 @@
 //     later calls; a lookup that fails is not kept, so the next call tries
 //     again. That first call should come before any stream capture begins
 //     on the device.
-// The kernels are the ones eaf_cg_solve_f64_device runs (pack, persistent
-// cooperative CG, unpack), launched with the same default shape, so results
+// The kernels are the ones eaf_cg_solve_f64_device runs (pack, the
+// persistent CG, unpack), launched with the same default shape, so results
 // are bit-identical to that entry point on the same inputs.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -34,6 +34,7 @@
 #include <mutex>
 
 #include "cg_kernels.h"
+#include "cluster_red.cuh"
 #include "eafcg.h"
 #include "eafcg_internal.h"
 #include "tune_table.h"
@@ -53,6 +54,11 @@ static_assert(eaf::max_tuned_grid_up_to(kNoallocMaxCells) <= kNoallocMaxBlocks,
 static_assert((kNoallocMaxCells + 2047) / 2048 <= kNoallocMaxBlocks,
               "the fallback launch shape exceeds the static scratch's block limit");
 constexpr int kPartSlots = 8;
+// A cluster launch uses the partial table as its slot table: at most
+// kNoallocMaxBlocks / 2 clusters of two or more blocks.
+static_assert(eaf::cluster_slot_doubles(kNoallocMaxBlocks / 2) <=
+                  (size_t)kPartSlots * kNoallocMaxBlocks,
+              "the partial table cannot hold the cluster all-reduce's slots");
 constexpr int kMaxDevices = 64;
 constexpr uint64_t kNoallocTimeoutNs = 2000ull * 1000ull * 1000ull;
 
@@ -93,16 +99,6 @@ cudaError_t scratch_on(int dev, double** out) {
   }
   *out = s.base;
   return cudaSuccess;
-}
-
-int max_coresident(int block, int dev) {
-  int per_sm = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eaf::cg_f64_kernel_ptr(block, 0),
-                                                    block, 0) != cudaSuccess)
-    return 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-    return 0;
-  return per_sm * sms;
 }
 
 }  // namespace
@@ -164,22 +160,18 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
   ws.err = reinterpret_cast<int*>(base + kErrOff);
   ws.result = reinterpret_cast<eaf::SolveResult*>(base + kResultOff);
 
-  // Launch shape: the default of eaf_cg_create handles (the tuned shape of
-  // the mesh; else one 1024-thread block up to 8192 cells or one 512-thread
-  // block per 2048 cells), capped by co-residency, so that results match the
+  // Launch: the default of eaf_cg_create handles on this mesh (tuned shape,
+  // cluster size and resident kernel included), so that results match the
   // handle entry points bit for bit.
-  int block = 512, grid;
-  if (eaf::tuned_single_launch(nr, nth, nz, &block, &grid)) {
-    // the tuned shape of this mesh, as the handle entry points use
-  } else if (n <= 8192) {
-    block = 1024;
-    grid = 1;
-  } else {
-    grid = (int)((n + 2047) / 2048);
+  int sms = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    eaf::set_error("eaf_cg_solve_f64_noalloc: cudaDeviceGetAttribute", e);
+    return EAF_ECUDA;
   }
-  const int cap = max_coresident(block, device);
-  if (cap > 0 && grid > cap) grid = cap;
-  if (grid > kNoallocMaxBlocks) {  // excluded by the static_asserts above
+  const eaf::SolverLaunch L =
+      eaf::choose_launch(nr, nth, nz, sms, 0, 0, 0, EAF_CG_FORM_REFERENCE, true);
+  if (L.grid > kNoallocMaxBlocks) {  // excluded by the static_asserts above
     eaf::set_error_text("eaf_cg_solve_f64_noalloc: launch shape exceeds the static scratch");
     return EAF_EINVAL;
   }
@@ -187,7 +179,8 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
   eaf::HaloInputs in = {aW, aE, aS, aN, aB, aT, aP, Su, phi};
   e = eaf::launch_pack_f64(d, in, s, st);
   if (e == cudaSuccess)
-    e = eaf::launch_cg_f64(d, s, ws, max_iter, tol, kNoallocTimeoutNs, grid, block, st);
+    e = eaf::launch_f64_solver(L, true, d, s, ws, (size_t)kPartSlots * kNoallocMaxBlocks,
+                               max_iter, tol, kNoallocTimeoutNs, st);
   if (e == cudaSuccess) e = eaf::launch_unpack_f64(d, s.x, phi, st);
   eaf::SolveResult r;
   if (e == cudaSuccess)

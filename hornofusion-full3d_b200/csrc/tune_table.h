@@ -26,31 +26,37 @@ inline int tuned_lane_width(int nr, int nth, int nz) {
 }
 
 struct TunedLaunch {
-  int nr, nth, nz, block, grid;
+  int nr, nth, nz, block, grid, cluster;
 };
 
-// (block, grid) of the single-system persistent solver.
+// (block, grid, blocks per cluster; 1 = no clusters) of the single-system
+// persistent solver.
 static constexpr TunedLaunch kTunedLaunches[] = {
-    {12, 24, 16, 256, 8},
-    {18, 36, 24, 256, 32},
-    {35, 70, 50, 256, 148},
-    {60, 120, 84, 512, 148},
-    {120, 240, 168, 1024, 148},
+    {12, 24, 16, 288, 16, 16},
+    {18, 36, 24, 512, 16, 16},
+    {35, 70, 50, 256, 148, 1},
+    {60, 120, 84, 512, 148, 1},
+    {120, 240, 168, 1024, 148, 1},
 };
 
-// Largest tuned grid among meshes of at most `max_cells` cells (0 if none).
+// Most blocks a tuned launch of a mesh of at most `max_cells` cells can run
+// (a grid is raised to one whole cluster at least); 0 if there is none.
 constexpr int max_tuned_grid_up_to(long long max_cells) {
   int g = 0;
-  for (const TunedLaunch& t : kTunedLaunches)
-    if ((long long)t.nr * t.nth * t.nz <= max_cells && t.grid > g) g = t.grid;
+  for (const TunedLaunch& t : kTunedLaunches) {
+    const int blocks = t.grid > t.cluster ? t.grid : t.cluster;
+    if ((long long)t.nr * t.nth * t.nz <= max_cells && blocks > g) g = blocks;
+  }
   return g;
 }
 
-inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid) {
+inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid,
+                                int* cluster = nullptr) {
   for (const TunedLaunch& t : kTunedLaunches)
     if (t.nr == nr && t.nth == nth && t.nz == nz) {
       *block = t.block;
       *grid = t.grid;
+      if (cluster) *cluster = t.cluster;
       return true;
     }
   return false;

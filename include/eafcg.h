@@ -128,6 +128,28 @@ int eaf_cg_get_launch(eaf_cg_t h, int* block_threads, int* grid_blocks);
  * dot products; the oracle's kernel-order mode takes the same shape). */
 int eaf_cg_last_launch(eaf_cg_t h, int* block_threads, int* grid_blocks);
 
+/* Thread-block clusters for the plain FP64 solve (reference form): blocks
+ * per cluster, 2..16, or 1 for none, or 0 for the tuned choice of the mesh.
+ * On a cluster grid each all-reduce folds the blocks' partials through the
+ * cluster leader's shared memory and only the leaders meet in global memory,
+ * so the dot products are associated per cluster (the oracle's plan
+ * (grid, block, cluster)); every other operation is unchanged. A size the
+ * device cannot launch falls back to none. No reference counterpart: the
+ * reference's dot is one sequential sum plus MPI_Allreduce
+ * (src/mod_solver_3d.f90:607-618). eaf_cg_get_cluster reports the size the
+ * next solve uses, eaf_cg_last_cluster the size the last one used. */
+int eaf_cg_set_cluster(eaf_cg_t h, int cluster_blocks);
+int eaf_cg_get_cluster(eaf_cg_t h, int* cluster_blocks);
+int eaf_cg_last_cluster(eaf_cg_t h, int* cluster_blocks);
+
+/* A launch that is ONE cluster (grid == cluster blocks) on a mesh that fits
+ * the cluster's shared memory (about 35,000 cells at 16 blocks) runs, by
+ * default (resident = 1), the cluster-resident kernel: the whole system
+ * lives in distributed shared memory for the whole solve and an iteration
+ * touches no global memory. It gives the same bits as the global-memory
+ * cluster kernel on that launch (resident = 0). No reference counterpart. */
+int eaf_cg_set_resident(eaf_cg_t h, int resident);
+
 /* Line-by-line TDMA on the handle's mesh: replaces tdma_3d_mpi
  * (src/mod_solver_3d.f90:252-366, serial branch; callers in momentum,
  * energy, species, k-epsilon, DO radiation and continuity, e.g.

@@ -41,6 +41,8 @@ def lib():
         L.eaf_oracle_cg_threads.restype = ci
         L.eaf_oracle_cg_tree.argtypes = (L.eaf_oracle_cg.argtypes + [ci, ci])
         L.eaf_oracle_cg_tree.restype = ci
+        L.eaf_oracle_cg_cluster.argtypes = (L.eaf_oracle_cg.argtypes + [ci, ci, ci])
+        L.eaf_oracle_cg_cluster.restype = ci
         L.eaf_oracle_cg1.argtypes = (L.eaf_oracle_cg.argtypes + [ci, ci])
         L.eaf_oracle_cg1.restype = ci
         L.eaf_oracle_dot.argtypes = [ci, ci, ci, _dp, _dp, ci, ci]
@@ -77,15 +79,18 @@ def cg(system, phi: np.ndarray, max_iter: int, tol: float, nthreads: int = 1,
     """Solve in place on ``phi`` (halo layout). Returns (residual, n_iter).
 
     ``plan=(G, B)`` associates the dot products as the CUDA kernels do for a
-    launch of G blocks x B threads (everything else is unchanged); the default
-    is the reference's sequential sum.
+    launch of G blocks x B threads (everything else is unchanged);
+    ``plan=(G, B, C)`` as the kernels do on a grid of thread-block clusters
+    of C blocks. The default is the reference's sequential sum.
     """
     res = ctypes.c_double(0.0)
     nit = ctypes.c_int(0)
     args = [system.nr, system.nth, system.nz] + [_p(a) for a in system.arrays()]
     args += [_p(phi), int(max_iter), float(tol), ctypes.byref(res),
              ctypes.byref(nit)]
-    if plan is not None:
+    if plan is not None and len(plan) > 2 and int(plan[2]) > 1:
+        rc = lib().eaf_oracle_cg_cluster(*args, int(plan[0]), int(plan[1]), int(plan[2]))
+    elif plan is not None:
         rc = lib().eaf_oracle_cg_tree(*args, int(plan[0]), int(plan[1]))
     elif nthreads == 1:
         rc = lib().eaf_oracle_cg(*args)

@@ -113,6 +113,7 @@ void eaf_oracle_theta_wrap(int nr, int nth, int nz, double* x) {
  * by the butterfly once more. */
 typedef struct {
     int G, B;
+    int C;  /* blocks per thread-block cluster (0 or 1: no clusters) */
 } plan_t;
 
 typedef struct {
@@ -191,14 +192,27 @@ static double dot_tree(const dims_t* d, const plan_t* pl, const double* a,
         }
         part[g] = block_tree(lane, B);
     }
+    /* Cluster grid (csrc/cluster_red.cuh): the leader of each cluster of C
+     * consecutive blocks folds their partials in rank order, starting from
+     * the first; the cluster partials then take the place of the block
+     * partials in the stage below (one cluster: its partial is the total). */
+    int np = G;
+    if (pl->C > 1) {
+        np = G / pl->C;
+        for (int c = 0; c < np; ++c) {
+            double cp = part[c * pl->C];
+            for (int r = 1; r < pl->C; ++r) cp = cp + part[c * pl->C + r];
+            part[c] = cp;
+        }
+    }
     double tot;
-    if (G == 1) {
+    if (np == 1) {
         tot = part[0];
     } else {
         double v[32];
         for (int l = 0; l < 32; ++l) {
             double s = 0.0;
-            for (int g = l; g < G; g += 32) s = s + part[g];
+            for (int g = l; g < np; g += 32) s = s + part[g];
             v[l] = s;
         }
         butterfly32(v);
@@ -250,6 +264,7 @@ static int cg_impl(int nr, int nth, int nz, const double* aW, const double* aE,
                    int* n_iter, int nthreads, plan_t plan) {
     if (nr < 1 || nth < 1 || nz < 1) return 2;
     if (plan.G < 0 || (plan.G > 0 && plan.B < 1)) return 2;
+    if (plan.C > 1 && (plan.G < plan.C || plan.G % plan.C != 0)) return 2;
     op_t o;
     o.plan = plan;
     o.d = mkdims(nr, nth, nz);
@@ -345,7 +360,7 @@ int eaf_oracle_cg(int nr, int nth, int nz, const double* aW, const double* aE,
                   const double* aT, const double* aP, const double* Su,
                   double* phi, int max_iter, double tol, double* residual,
                   int* n_iter) {
-    plan_t seq = {0, 0};
+    plan_t seq = {0, 0, 0};
     return cg_impl(nr, nth, nz, aW, aE, aS, aN, aB, aT, aP, Su, phi, max_iter,
                    tol, residual, n_iter, 1, seq);
 }
@@ -360,7 +375,21 @@ int eaf_oracle_cg_tree(int nr, int nth, int nz, const double* aW,
                        const double* Su, double* phi, int max_iter, double tol,
                        double* residual, int* n_iter, int G, int B) {
     if (G < 1 || B < 1) return 2;
-    plan_t pl = {G, B};
+    plan_t pl = {G, B, 0};
+    return cg_impl(nr, nth, nz, aW, aE, aS, aN, aB, aT, aP, Su, phi, max_iter,
+                   tol, residual, n_iter, 1, pl);
+}
+
+/* The same with the launch on a grid of thread-block clusters of C blocks
+ * (G a multiple of C): the dots are associated per cluster as the cluster
+ * all-reduce does (see dot_tree). C <= 1 is eaf_oracle_cg_tree. */
+int eaf_oracle_cg_cluster(int nr, int nth, int nz, const double* aW,
+                          const double* aE, const double* aS, const double* aN,
+                          const double* aB, const double* aT, const double* aP,
+                          const double* Su, double* phi, int max_iter, double tol,
+                          double* residual, int* n_iter, int G, int B, int C) {
+    if (G < 1 || B < 1 || C < 0) return 2;
+    plan_t pl = {G, B, C};
     return cg_impl(nr, nth, nz, aW, aE, aS, aN, aB, aT, aP, Su, phi, max_iter,
                    tol, residual, n_iter, 1, pl);
 }
@@ -389,6 +418,7 @@ static int cg1_impl(int nr, int nth, int nz, const double* aW, const double* aE,
                     int* n_iter, plan_t plan) {
     if (nr < 1 || nth < 1 || nz < 1) return 2;
     if (plan.G < 0 || (plan.G > 0 && plan.B < 1)) return 2;
+    if (plan.C > 1 && (plan.G < plan.C || plan.G % plan.C != 0)) return 2;
     op_t o;
     o.plan = plan;
     o.d = mkdims(nr, nth, nz);
@@ -480,7 +510,7 @@ int eaf_oracle_cg1(int nr, int nth, int nz, const double* aW, const double* aE,
                    const double* aT, const double* aP, const double* Su,
                    double* phi, int max_iter, double tol, double* residual,
                    int* n_iter, int G, int B) {
-    plan_t pl = {G, B};
+    plan_t pl = {G, B, 0};
     return cg1_impl(nr, nth, nz, aW, aE, aS, aN, aB, aT, aP, Su, phi, max_iter,
                     tol, residual, n_iter, pl);
 }
@@ -495,6 +525,7 @@ double eaf_oracle_dot(int nr, int nth, int nz, const double* a, const double* b,
     o.nthreads = 1;
     o.plan.G = G;
     o.plan.B = B;
+    o.plan.C = 0;
     return dot(&o, a, b);
 }
 
@@ -506,7 +537,7 @@ int eaf_oracle_cg_threads(int nr, int nth, int nz, const double* aW,
                           const double* Su, double* phi, int max_iter,
                           double tol, double* residual, int* n_iter,
                           int nthreads) {
-    plan_t seq = {0, 0};
+    plan_t seq = {0, 0, 0};
     return cg_impl(nr, nth, nz, aW, aE, aS, aN, aB, aT, aP, Su, phi, max_iter,
                    tol, residual, n_iter, nthreads < 1 ? 1 : nthreads, seq);
 }
@@ -523,6 +554,7 @@ void eaf_oracle_matvec(int nr, int nth, int nz, const double* aW,
     o.nthreads = 1;
     o.plan.G = 0;
     o.plan.B = 0;
+    o.plan.C = 0;
     matvec(&o, x, y);
 }
 
