@@ -415,6 +415,7 @@ def run_fine(args):
                                          max_outer=args.mixed_outer,
                                          max_inner=args.mixed_inner, device_ptrs=True)
         tm = cg.last_timing()
+        trace = cg.mixed_trace(args.mixed_outer)
         xm = phim.cpu().numpy()
     I = g.interior
     err = float(np.linalg.norm(I(xm) - I(x64)) / np.linalg.norm(I(x64)))
@@ -435,7 +436,8 @@ def run_fine(args):
                      "outer_steps": no, "kernel_ms": tm["kernel_ms"],
                      "caps": {"max_outer": args.mixed_outer, "max_inner": args.mixed_inner},
                      "rel_l2_error_vs_fp64": err,
-                     "fp64_kernel_ms_per_solve": kms / args.steps}
+                     "fp64_kernel_ms_per_solve": kms / args.steps,
+                     "trace": trace}
     print(json.dumps(line), flush=True)
     return 0
 

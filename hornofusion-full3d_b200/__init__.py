@@ -276,6 +276,32 @@ class CGSolver:
         kernel; both give the same bits."""
         check(self._lib.eaf_cg_set_resident(self._h, int(bool(resident))), "set_resident")
 
+    def mixed_trace(self, max_steps: int = 1000) -> list:
+        """Per refinement step of the last mixed-precision solve: inner FP32
+        iterations, the inner CG's residual reduction and the FP64 outer
+        residual after the step."""
+        buf = (ctypes.c_double * (3 * max_steps))()
+        n = ctypes.c_int()
+        check(self._lib.eaf_cg_mixed_trace(self._h, buf, int(max_steps), ctypes.byref(n)),
+              "mixed_trace")
+        return [{"inner_iterations": int(buf[3 * k]), "inner_reduction": buf[3 * k + 1],
+                 "residual": buf[3 * k + 2]} for k in range(n.value)]
+
+    KERNEL_AUTO = 0
+    KERNEL_LOADS = 1
+    KERNEL_STREAM = 2
+
+    def set_kernel(self, kernel: int = 0) -> None:
+        """Kernel of the plain FP64 solve on a flat grid: KERNEL_LOADS
+        (per-thread loads), KERNEL_STREAM (bulk-copy staging) or KERNEL_AUTO
+        (the tuned choice); the same bits either way."""
+        check(self._lib.eaf_cg_set_kernel(self._h, int(kernel)), "set_kernel")
+
+    def last_kernel(self) -> int:
+        k = ctypes.c_int()
+        check(self._lib.eaf_cg_last_kernel(self._h, ctypes.byref(k)), "last_kernel")
+        return k.value
+
     def cluster(self) -> int:
         """Blocks per cluster the next plain FP64 solve runs with."""
         c = ctypes.c_int()

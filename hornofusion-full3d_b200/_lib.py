@@ -128,6 +128,9 @@ SIGNATURES = [
     ("eaf_cg_get_cluster", _ci, [_vp, _pi]),
     ("eaf_cg_last_cluster", _ci, [_vp, _pi]),
     ("eaf_cg_set_resident", _ci, [_vp, _ci]),
+    ("eaf_cg_set_kernel", _ci, [_vp, _ci]),
+    ("eaf_cg_mixed_trace", _ci, [_vp, _vp, _ci, _pi]),
+    ("eaf_cg_last_kernel", _ci, [_vp, _pi]),
     ("eaf_cg_last_timing", _ci, [_vp, _pd, _pd, _pi, _pi]),
     ("eaf_cg_last_e2e_ms", _cd, [_vp]),
     ("eaf_cg_stream", _vp, [_vp]),

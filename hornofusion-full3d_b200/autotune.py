@@ -51,7 +51,8 @@ def select(log):
         sm = [m for m in log if tuple(m["mesh"]) == d and m["solver"] == "single"]
         if sm:
             b = min(sm, key=lambda m: (m["us_per_iter"], m["block"], m["grid"]))
-            single.append((d, b["block"], b["grid"], b.get("cluster", 1), b["us_per_iter"]))
+            single.append((d, b["block"], b["grid"], b.get("cluster", 1), b.get("stream", 0),
+                           b["us_per_iter"]))
         lm = [m for m in log if tuple(m["mesh"]) == d and m["solver"] == "lane"]
         if lm:
             tmin = min(m["us_per_iter"] for m in lm)
@@ -61,10 +62,11 @@ def select(log):
     return single, lanes
 
 
-def time_single(eaf, dev_arrays, phi, dims, block, grid, iters, cluster=1):
+def time_single(eaf, dev_arrays, phi, dims, block, grid, iters, cluster=1, stream=0):
     with eaf.CGSolver(*dims) as cg:
         cg.set_launch(block, grid)
         cg.set_cluster(cluster)
+        cg.set_kernel(cg.KERNEL_STREAM if stream else cg.KERNEL_LOADS)
         best = float("inf")
         for _ in range(2):
             phi.zero_()
@@ -98,8 +100,8 @@ def main(argv=None) -> int:
         with open(args.from_json) as f:
             res = json.load(f)
         single, lanes = select(res["measurements"])
-        res["single"] = [{"mesh": list(d), "block": b, "grid": gr, "cluster": c,
-                          "us_per_iter": u} for d, b, gr, c, u in single]
+        res["single"] = [{"mesh": list(d), "block": b, "grid": gr, "cluster": c, "stream": st,
+                          "us_per_iter": u} for d, b, gr, c, st, u in single]
         res["lanes"] = [{"mesh": list(d), "width": w, "us_per_iter": u}
                         for d, w, u in lanes]
         res["lane_rule"] = f"least t(w)*w among t(w) <= {LATENCY_SLACK} x min t"
@@ -132,6 +134,10 @@ def main(argv=None) -> int:
             us, used = time_single(eaf, dev, phi, dims, block, grid, args.iters)
             log.append({"mesh": dims, "solver": "single", "block": block, "grid": used[0],
                         "us_per_iter": round(us, 3)})
+        for block in (512, 1024):  # the bulk-copy streaming kernel, one block per SM
+            us, used = time_single(eaf, dev, phi, dims, block, sms, args.iters, 1, 1)
+            log.append({"mesh": dims, "solver": "single", "block": block, "grid": used[0],
+                        "stream": 1, "us_per_iter": round(us, 3)})
         if n <= RESIDENT_MAX_CELLS:  # one cluster holding the system on chip
             for c in (4, 8, 16):
                 for block in (128, 256, 288, 512, 1024):
@@ -151,8 +157,8 @@ def main(argv=None) -> int:
     single, lanes = select(log)
     result = {"gpu": torch.cuda.get_device_name(0), "iters": args.iters,
               "lane_rule": f"least t(w)*w among t(w) <= {LATENCY_SLACK} x min t",
-              "single": [{"mesh": d, "block": b, "grid": gr, "cluster": c,
-                          "us_per_iter": round(u, 3)} for d, b, gr, c, u in single],
+              "single": [{"mesh": d, "block": b, "grid": gr, "cluster": c, "stream": st,
+                          "us_per_iter": round(u, 3)} for d, b, gr, c, st, u in single],
               "lanes": [{"mesh": d, "width": w, "us_per_iter": round(u, 3)}
                         for d, w, u in lanes],
               "measurements": log}
@@ -170,8 +176,8 @@ def main(argv=None) -> int:
 
 def write_header(single, lanes, path):
     rows_l = "\n".join(f"    {{{d[0]}, {d[1]}, {d[2]}, {w}}}," for d, w, _ in lanes)
-    rows_s = "\n".join(f"    {{{d[0]}, {d[1]}, {d[2]}, {b}, {gr}, {c}}},"
-                       for d, b, gr, c, _ in single)
+    rows_s = "\n".join(f"    {{{d[0]}, {d[1]}, {d[2]}, {b}, {gr}, {c}, {st}}},"
+                       for d, b, gr, c, st, _ in single)
     text = f"""// Launch shapes measured on B200 by hornofusion-full3d_b200/autotune.py
 // (tune_table.json beside it holds every measurement). Meshes that are not
 // in a table fall back to the rules below.
@@ -197,11 +203,11 @@ inline int tuned_lane_width(int nr, int nth, int nz) {{
 }}
 
 struct TunedLaunch {{
-  int nr, nth, nz, block, grid, cluster;
+  int nr, nth, nz, block, grid, cluster, stream;
 }};
 
-// (block, grid, blocks per cluster; 1 = no clusters) of the single-system
-// persistent solver.
+// (block, grid, blocks per cluster (1 = no clusters), bulk-copy streaming
+// kernel (1) or per-thread loads (0)) of the single-system persistent solver.
 static constexpr TunedLaunch kTunedLaunches[] = {{
 {rows_s}
 }};
@@ -218,12 +224,13 @@ constexpr int max_tuned_grid_up_to(long long max_cells) {{
 }}
 
 inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid,
-                                int* cluster = nullptr) {{
+                                int* cluster = nullptr, int* stream = nullptr) {{
   for (const TunedLaunch& t : kTunedLaunches)
     if (t.nr == nr && t.nth == nth && t.nz == nz) {{
       *block = t.block;
       *grid = t.grid;
       if (cluster) *cluster = t.cluster;
+      if (stream) *stream = t.stream;
       return true;
     }}
   return false;

@@ -80,6 +80,7 @@ static void free_handle(eaf_cg* h) {
   cudaFree(h->asm_d);
   cudaFree(h->asm_i);
   cudaFree(h->asm_s);
+  cudaFree(h->trace_d);
   for (int i = 0; i < 2; ++i)
     if (h->step_ev[i]) cudaEventDestroy(h->step_ev[i]);
   if (h->res_h) cudaFreeHost(h->res_h);
@@ -107,7 +108,7 @@ namespace eaf {
 // the grid is then a whole number of clusters, at most as many as can be
 // resident; a cluster size the device cannot launch falls back to none.
 SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int req_grid,
-                           int req_cluster, int form, bool f64) {
+                           int req_cluster, int form, bool f64, int req_kernel) {
   const long long n = (long long)nr * nth * nz;
   auto kernel_for = [f64, form, n](int b) {
     if (!f64) return cg_mixed_kernel_ptr();
@@ -115,9 +116,9 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
   };
   int b = req_block > 0 ? req_block : kDefaultBlock;
   int g;
-  int tb = 0, tg = 0, tc = 1;
+  int tb = 0, tg = 0, tc = 1, ts = 0;
   const bool automatic = req_block == 0 && req_grid == 0;
-  if (automatic && f64 && tuned_single_launch(nr, nth, nz, &tb, &tg, &tc)) {
+  if (automatic && f64 && tuned_single_launch(nr, nth, nz, &tb, &tg, &tc, &ts)) {
     b = tb;
     g = tg;
   } else if (req_grid > 0) {
@@ -146,8 +147,16 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
       }
     }
   }
+  int stream = 0;
+  if (f64 && form == EAF_CG_FORM_REFERENCE && c == 1) {
+    stream = req_kernel == EAF_CG_KERNEL_STREAM ? 1
+             : req_kernel == EAF_CG_KERNEL_LOADS ? 0
+                                                 : (automatic ? ts : 0);
+    if (stream && (b % 32 != 0 || stream_max_coresident(b, nr, sms) < 1)) stream = 0;
+  }
   if (c == 1) {
-    const int cap = max_coresident(kernel_for(b), b, sms);
+    const int cap = stream ? stream_max_coresident(b, nr, sms)
+                           : max_coresident(kernel_for(b), b, sms);
     if (cap > 0 && g > cap) g = cap;
     if (g > sms * 8) g = sms * 8;
   }
@@ -155,6 +164,7 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
   L.grid = g;
   L.block = b;
   L.cluster = c;
+  L.stream = stream;
   return L;
 }
 
@@ -170,17 +180,22 @@ cudaError_t launch_f64_solver(const SolverLaunch& L, bool resident, const MeshDi
   if (L.cluster > 1)
     return launch_cg_f64_cluster(d, s, ws, ws.part, slot_doubles, max_iter, tol, timeout_ns,
                                  L.grid, L.block, L.cluster, st);
+  if (L.stream)
+    return launch_cg_f64_stream(d, s, ws, max_iter, tol, timeout_ns, L.grid, L.block, st);
   return launch_cg_f64(d, s, ws, max_iter, tol, timeout_ns, L.grid, L.block, st);
 }
 
 }  // namespace eaf
 
-static void pick_launch(const eaf_cg* h, bool f64, int* grid, int* block, int* cluster) {
+static eaf::SolverLaunch pick_launch(const eaf_cg* h, bool f64, int* grid, int* block,
+                                     int* cluster) {
   const eaf::SolverLaunch L = eaf::choose_launch(h->nr, h->nth, h->nz, h->sms, h->block,
-                                                 h->grid, h->cluster, h->form, f64);
+                                                 h->grid, h->cluster, h->form, f64,
+                                                 h->kernel);
   *grid = L.grid;
   *block = L.block;
   *cluster = L.cluster;
+  return L;
 }
 
 extern "C" {
@@ -241,7 +256,9 @@ int eaf_cg_create_mesh(eaf_cg_t* out, int nr, int nth, int nz, int is_parallel,
                     &h->s.aS, &h->s.aB, &h->s.b,  &h->s.x,  &h->s.r,
                     &h->s.p,  &h->s.q,  &h->s.p2, &h->s.z, &h->s.s0, &h->s.s1,
                     &h->s.dinv};
-  for (double** p : f64) alloc((void**)p, (size_t)n * sizeof(double));
+  // One padding cell (two, rounded) past each compact array: the streaming
+  // kernel's bulk copies move whole 16-byte pairs of cells.
+  for (double** p : f64) alloc((void**)p, (size_t)(n + 2) * sizeof(double));
   alloc((void**)&h->s.asym, sizeof(int));
   int dev_sms = 0;
   if (e == cudaSuccess)
@@ -314,6 +331,31 @@ int eaf_cg_get_cluster(eaf_cg_t h, int* cluster_blocks) {
   eaf::DeviceGuard guard(h->device);
   int grid = 0, block = 0;
   pick_launch(h, true, &grid, &block, cluster_blocks);
+  return EAF_OK;
+}
+
+int eaf_cg_mixed_trace(eaf_cg_t h, double* steps, int max_steps, int* n_steps) {
+  if (!h || !n_steps || max_steps < 0 || (max_steps > 0 && !steps)) return EAF_EINVAL;
+  eaf::DeviceGuard guard(h->device);
+  int n = h->res_h ? h->res_h->n_outer : 0;
+  if (n > h->trace_cap) n = h->trace_cap;
+  if (n > max_steps) n = max_steps;
+  *n_steps = n;
+  if (n > 0)
+    EAF_CUDA(cudaMemcpy(steps, h->trace_d, sizeof(double) * 3 * (size_t)n,
+                        cudaMemcpyDeviceToHost));
+  return EAF_OK;
+}
+
+int eaf_cg_set_kernel(eaf_cg_t h, int kernel) {
+  if (!h || kernel < EAF_CG_KERNEL_AUTO || kernel > EAF_CG_KERNEL_STREAM) return EAF_EINVAL;
+  h->kernel = kernel;
+  return EAF_OK;
+}
+
+int eaf_cg_last_kernel(eaf_cg_t h, int* kernel) {
+  if (!h || !kernel) return EAF_EINVAL;
+  *kernel = h->last_stream ? EAF_CG_KERNEL_STREAM : EAF_CG_KERNEL_LOADS;
   return EAF_OK;
 }
 
@@ -425,19 +467,26 @@ int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts&
     int rc = ensure_f32(h);
     if (rc != EAF_OK) return rc;
     pick_launch(h, false, &grid, &block, &cluster);
+    if (o.max_outer > h->trace_cap) {
+      cudaFree(h->trace_d);
+      h->trace_d = nullptr;
+      h->trace_cap = 0;
+      EAF_CUDA(cudaMalloc((void**)&h->trace_d, sizeof(double) * 3 * (size_t)o.max_outer));
+      h->trace_cap = o.max_outer;
+    }
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     EAF_CUDA(eaf::launch_cg_mixed(h->d, h->s, h->f, h->ws, o.max_outer, o.max_iter,
                                   o.tol, o.inner_tol, h->timeout_ns, grid, block,
-                                  h->st));
+                                  h->st, h->trace_d));
   } else {
-    pick_launch(h, true, &grid, &block, &cluster);
+    const eaf::SolverLaunch L = pick_launch(h, true, &grid, &block, &cluster);
+    h->last_stream = L.stream;
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     if (h->form == EAF_CG_FORM_ONE_REDUCTION)
       EAF_CUDA(eaf::launch_cg1_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
                                    grid, block, h->st));
     else
-      EAF_CUDA(eaf::launch_f64_solver(eaf::SolverLaunch{grid, block, cluster},
-                                      h->resident != 0, h->d, h->s, h->ws,
+      EAF_CUDA(eaf::launch_f64_solver(L, h->resident != 0, h->d, h->s, h->ws,
                                       kPartTableDoubles(h), o.max_iter, o.tol,
                                       h->timeout_ns, h->st));
   }

@@ -21,6 +21,7 @@
 #include "cg_kernels.h"
 #include "cluster_red.cuh"
 #include "stencil.cuh"
+#include "stream_stage.cuh"
 
 namespace eaf {
 
@@ -305,6 +306,363 @@ __global__ void __launch_bounds__(MAXB, 1) cg_cluster_kernel(CgArgs a, double* s
   // No block leaves while another block of its cluster may still address
   // its shared memory.
   cluster_sync_all();
+}
+
+// ---------------------------------------------------------------------------
+// Streaming form: the same solver with every phase's operands staged in
+// shared memory by bulk copies (stream_stage.cuh), a few tiles ahead of the
+// threads that use them. A block walks its slice in tiles of B cells (one
+// cell per thread per tile, so thread t visits the cells it visits in
+// cg_body, in the same order: the dot products, the per-cell arithmetic and
+// the result are bit-identical to cg_f64_kernel on the same launch). For
+// the stencil phase a tile's stage holds, for cells [t0, t1):
+//   the direction inputs (z and the old direction, or p in iteration 1) over
+//   [t0 - nr, t1 + nr) (own cells, r and theta neighbours) and over the
+//   tiles one z-plane below and above (the bottom and top neighbours),
+//   aN over [t0 - nr, t1), aE over [t0 - 1, t1), aP and aT over the tile and
+//   aT one plane below;
+// only the theta-periodic wrap neighbours (j = 0 and j = nth - 1) are read
+// from global memory directly. The update phase stages p, q, aP, x and r of
+// the tile. Results go to global memory with ordinary stores, followed by a
+// proxy fence so that the next phase's bulk copies (async proxy) see them
+// once the all-reduce has published them. Symmetric (4-array) operators
+// only; the 7-array form runs cg_body's per-thread loads in the same
+// kernel.
+// ---------------------------------------------------------------------------
+constexpr int kMaxStages = 4;
+
+struct StreamLayout {
+  int S;      // stages
+  int wc;     // capacity (doubles) of a centre window: B + 2 nr + 4
+  int wb;     // capacity of a tile window: B + 4
+  int stage;  // doubles per stage
+};
+
+__host__ __device__ __forceinline__ StreamLayout stream_layout(int B, int nr, int S) {
+  StreamLayout L;
+  L.S = S;
+  L.wc = B + 2 * nr + 4;
+  L.wb = B + 4;
+  L.stage = 3 * L.wc + 8 * L.wb;
+  return L;
+}
+
+// Stage slot offsets (doubles) of the stencil phase.
+enum { kSzc, kSzd, kSzu, kSoc, kSod, kSou, kSaN, kSaE, kSaP, kSaT, kSaTd, kSlots };
+__device__ __forceinline__ int slot_off(const StreamLayout& L, int k) {
+  // zc, zd, zu, oc, od, ou, aN, aE, aP, aT, aTd
+  const int wc = L.wc, wb = L.wb;
+  switch (k) {
+    case kSzc: return 0;
+    case kSzd: return wc;
+    case kSzu: return wc + wb;
+    case kSoc: return wc + 2 * wb;
+    case kSod: return 2 * wc + 2 * wb;
+    case kSou: return 2 * wc + 3 * wb;
+    case kSaN: return 2 * wc + 4 * wb;
+    case kSaE: return 3 * wc + 4 * wb;
+    case kSaP: return 3 * wc + 5 * wb;
+    case kSaT: return 3 * wc + 6 * wb;
+    default: return 3 * wc + 7 * wb;  // kSaTd
+  }
+}
+
+struct StencilTile {
+  Window zc, zd, zu, oc, od, ou, aN, aE, aP, aT, aTd;
+};
+
+// Windows of the stencil phase for tile [t0, t1) (bounds rounded out to even
+// cells; the plane-shifted windows are empty where they leave the mesh).
+__device__ __forceinline__ StencilTile stencil_tile(const StreamLayout& L, double* st,
+                                                   const MeshDims& d, int t0, int t1) {
+  StencilTile T;
+  const int n = d.n, nr = d.nr, pl = d.plane;
+  const int cl = even_floor(max(t0 - nr, 0)), ch = even_ceil(min(t1 + nr, n));
+  int dl = even_floor(max(t0 - pl, 0)), dh = even_ceil(max(t1 - pl, 0));
+  if (dh < dl) dh = dl;
+  int ul = even_floor(min(t0 + pl, n)), uh = even_ceil(min(t1 + pl, n));
+  if (uh < ul) uh = ul;
+  const int el = even_floor(max(t0 - 1, 0)), tl = even_floor(t0), th = even_ceil(t1);
+  T.zc = {st + slot_off(L, kSzc), cl, ch};
+  T.zd = {st + slot_off(L, kSzd), dl, dh};
+  T.zu = {st + slot_off(L, kSzu), ul, uh};
+  T.oc = {st + slot_off(L, kSoc), cl, ch};
+  T.od = {st + slot_off(L, kSod), dl, dh};
+  T.ou = {st + slot_off(L, kSou), ul, uh};
+  T.aN = {st + slot_off(L, kSaN), cl, th};
+  T.aE = {st + slot_off(L, kSaE), el, th};
+  T.aP = {st + slot_off(L, kSaP), tl, th};
+  T.aT = {st + slot_off(L, kSaT), tl, th};
+  T.aTd = {st + slot_off(L, kSaTd), dl, dh};
+  return T;
+}
+
+__device__ __forceinline__ uint32_t copy_window(const Window& w, const double* src,
+                                                uint64_t* bar) {
+  const int cells = w.hi - w.lo;
+  if (cells <= 0) return 0u;
+  bulk_copy_g2s((void*)w.buf, src + w.lo, 8u * (uint32_t)cells, bar);
+  return 8u * (uint32_t)cells;
+}
+
+__device__ __forceinline__ uint32_t window_bytes(const Window& w) {
+  return w.hi > w.lo ? 8u * (uint32_t)(w.hi - w.lo) : 0u;
+}
+
+// Issues the stencil-phase copies of one tile (thread 0 only). `x` is the
+// direction input (z, or p in iteration 1), `o` the old direction (nullptr
+// in iteration 1).
+__device__ void issue_stencil(const StreamLayout& L, double* st, uint64_t* bar,
+                              const MeshDims& d, const SysF64& s, const double* x,
+                              const double* o, int t0, int t1) {
+  const StencilTile T = stencil_tile(L, st, d, t0, t1);
+  uint32_t bytes = window_bytes(T.zc) + window_bytes(T.zd) + window_bytes(T.zu) +
+                   window_bytes(T.aN) + window_bytes(T.aE) + window_bytes(T.aP) +
+                   window_bytes(T.aT) + window_bytes(T.aTd);
+  if (o) bytes += window_bytes(T.oc) + window_bytes(T.od) + window_bytes(T.ou);
+  mbar_arrive_expect(bar, bytes);
+  copy_window(T.zc, x, bar);
+  copy_window(T.zd, x, bar);
+  copy_window(T.zu, x, bar);
+  if (o) {
+    copy_window(T.oc, o, bar);
+    copy_window(T.od, o, bar);
+    copy_window(T.ou, o, bar);
+  }
+  copy_window(T.aN, s.aN, bar);
+  copy_window(T.aE, s.aE, bar);
+  copy_window(T.aP, s.aP, bar);
+  copy_window(T.aT, s.aT, bar);
+  copy_window(T.aTd, s.aT, bar);
+}
+
+// Update phase: p, q, aP, x, r of the tile.
+__device__ __forceinline__ Window update_window(const StreamLayout& L, double* st, int k,
+                                                int t0, int t1) {
+  return Window{st + k * L.wb, even_floor(t0), even_ceil(t1)};
+}
+
+__device__ void issue_update(const StreamLayout& L, double* st, uint64_t* bar,
+                             const SysF64& s, const double* p, int t0, int t1) {
+  const Window w = update_window(L, st, 0, t0, t1);
+  mbar_arrive_expect(bar, 5u * window_bytes(w));
+  const double* src[5] = {p, s.q, s.aP, s.x, s.r};
+#pragma unroll
+  for (int k = 0; k < 5; ++k) copy_window(update_window(L, st, k, t0, t1), src[k], bar);
+}
+
+// Waits for every tile issued but not consumed (after a failed wait), so
+// that no copy into this block's shared memory is in flight when it leaves.
+__device__ void drain_stages(uint64_t* bars, uint32_t& par, int S, int from, int to,
+                             int* err, uint64_t timeout_ns) {
+  if (threadIdx.x == 0) {
+    for (int t = from; t < to; ++t) {
+      const int sidx = t % S;
+      mbar_wait(&bars[sidx], (par >> sidx) & 1u, err, timeout_ns);
+      par ^= 1u << sidx;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ void cg_stream_body(const CgArgs& a, Group& g, double* smem, uint64_t* bars,
+                               const StreamLayout& L) {
+  const MeshDims& d = a.d;
+  const SysF64& s = a.s;
+  const Slice own = own_slice(d.n, g.nb, g.bid);
+  const Coefs<double> A = coefs_of<double>(s.aP, s.aE, s.aN, s.aT, s.aW, s.aS, s.aB);
+  const double* __restrict__ aP = s.aP;
+  const double* __restrict__ b = s.b;
+  double* __restrict__ x = s.x;
+  double* __restrict__ r = s.r;
+  double* __restrict__ z = s.z;
+  double* __restrict__ q = s.q;
+  const int B = blockDim.x;
+  const int S = L.S;
+  const int ntile = own.end > own.begin ? (own.end - own.begin + B - 1) / B : 0;
+  uint32_t par = 0;  // expected completion parity of each stage
+
+  // Preamble (src/mod_solver_3d.f90:515-530) with per-thread loads, as cg_body.
+  double v3[3] = {0.0, 0.0, 0.0};
+  for (int c = own.begin + (int)threadIdx.x; c < own.end; c += B) {
+    const double bv = b[c], rv = r[c];
+    const double zv = rv / guard_small(fabs(aP[c]));
+    s.p[c] = zv;
+    v3[0] = v3[0] + bv * bv;
+    v3[1] = v3[1] + rv * rv;
+    v3[2] = v3[2] + rv * zv;
+  }
+  fence_proxy_async_global();
+  bool ok = allsum<3>(v3, g, 0);
+  const double bnorm = sqrt(v3[0]);
+  double residual = 0.0;
+  int n_iter = 0;
+  bool nan_fill = false;
+  if (ok && !(bnorm < kSmall)) {
+    double rz = v3[2];
+    double beta = 0.0;
+    residual = sqrt(v3[1]) / bnorm;
+    if (residual != residual && a.max_iter >= 1) nan_fill = true;
+    for (int iter = 1; iter <= a.max_iter && !nan_fill; ++iter) {
+      const double* __restrict__ pold = (iter & 1) ? s.p2 : s.p;
+      double* __restrict__ pcur = (iter & 1) ? s.p : s.p2;
+      const bool first = iter == 1;
+      const double* xin = first ? pcur : z;
+      const double* oin = first ? nullptr : pold;
+      const double bt = beta;
+      // Phase A: p = z + beta p_old, q = A p, p.q (tiles of B cells).
+      double v1[1] = {0.0};
+      if (threadIdx.x == 0) {
+        for (int t = 0; t < S && t < ntile; ++t) {
+          const int t0 = own.begin + t * B;
+          issue_stencil(L, smem + (size_t)t * L.stage, &bars[t], d, s, xin, oin, t0,
+                        min(t0 + B, own.end));
+        }
+      }
+      for (int t = 0; t < ntile; ++t) {
+        const int sidx = t % S;
+        double* st = smem + (size_t)sidx * L.stage;
+        const int t0 = own.begin + t * B, t1 = min(t0 + B, own.end);
+        bool w_ok = mbar_wait(&bars[sidx], (par >> sidx) & 1u, g.err, g.timeout_ns);
+        par ^= 1u << sidx;
+        const int c = t0 + (int)threadIdx.x;
+        if (w_ok && c < t1) {
+          const StencilTile T = stencil_tile(L, st, d, t0, t1);
+          int i, j, k;
+          cell_ijk(d, c, i, j, k);
+          auto xv = [&](const Window& wz, const Window& wo, int cc) {
+            return first ? wz[cc] : wz[cc] + bt * wo[cc];
+          };
+          auto xg = [&](int cc) { return first ? xin[cc] : xin[cc] + bt * oin[cc]; };
+          const double pc = xv(T.zc, T.oc, c);
+          double y = T.aP[c] * pc;
+          if (i > 0) y = y - T.aE[c - 1] * xv(T.zc, T.oc, c - 1);
+          if (i < d.nr - 1) y = y - T.aE[c] * xv(T.zc, T.oc, c + 1);
+          if (j > 0) {
+            y = y - T.aN[c - d.nr] * xv(T.zc, T.oc, c - d.nr);
+          } else {
+            const int cs = c + (d.nth - 1) * d.nr;
+            y = y - A.aN[cs] * xg(cs);
+          }
+          if (j < d.nth - 1)
+            y = y - T.aN[c] * xv(T.zc, T.oc, c + d.nr);
+          else
+            y = y - T.aN[c] * xg(c - (d.nth - 1) * d.nr);
+          if (k > 0) y = y - T.aTd[c - d.plane] * xv(T.zd, T.od, c - d.plane);
+          if (k < d.nz - 1) y = y - T.aT[c] * xv(T.zu, T.ou, c + d.plane);
+          if (!first) pcur[c] = pc;
+          q[c] = y;
+          v1[0] = v1[0] + pc * y;
+        }
+        ok = __syncthreads_and(w_ok) != 0;
+        if (!ok) {
+          drain_stages(bars, par, S, t + 1, min(t + S, ntile), g.err, g.timeout_ns);
+          break;
+        }
+        if (threadIdx.x == 0 && t + S < ntile) {
+          const int n0 = own.begin + (t + S) * B;
+          issue_stencil(L, st, &bars[sidx], d, s, xin, oin, n0, min(n0 + B, own.end));
+        }
+      }
+      if (!ok) break;
+      fence_proxy_async_global();
+      if (!(ok = allsum<1>(v1, g, 3))) break;
+      const double pq = v1[0];
+      if (fabs(pq) < kSmall) break;
+      const double alpha = rz / pq;
+      // Phase B: phi += alpha pv; r -= alpha q; r.r; z and r.z (:538-553)
+      double v2[2] = {0.0, 0.0};
+      if (threadIdx.x == 0) {
+        for (int t = 0; t < S && t < ntile; ++t) {
+          const int t0 = own.begin + t * B;
+          issue_update(L, smem + (size_t)t * L.stage, &bars[t], s, pcur, t0,
+                       min(t0 + B, own.end));
+        }
+      }
+      for (int t = 0; t < ntile; ++t) {
+        const int sidx = t % S;
+        double* st = smem + (size_t)sidx * L.stage;
+        const int t0 = own.begin + t * B, t1 = min(t0 + B, own.end);
+        bool w_ok = mbar_wait(&bars[sidx], (par >> sidx) & 1u, g.err, g.timeout_ns);
+        par ^= 1u << sidx;
+        const int c = t0 + (int)threadIdx.x;
+        if (w_ok && c < t1) {
+          const double pv = update_window(L, st, 0, t0, t1)[c];
+          const double qv = update_window(L, st, 1, t0, t1)[c];
+          const double dv = update_window(L, st, 2, t0, t1)[c];
+          const double xv0 = update_window(L, st, 3, t0, t1)[c];
+          const double rv = update_window(L, st, 4, t0, t1)[c];
+          const double xn = xv0 + alpha * pv;
+          const double rn = rv - alpha * qv;
+          const double zv = rn / guard_small(fabs(dv));
+          x[c] = xn;
+          r[c] = rn;
+          z[c] = zv;
+          v2[0] = v2[0] + rn * rn;
+          v2[1] = v2[1] + rn * zv;
+        }
+        ok = __syncthreads_and(w_ok) != 0;
+        if (!ok) {
+          drain_stages(bars, par, S, t + 1, min(t + S, ntile), g.err, g.timeout_ns);
+          break;
+        }
+        if (threadIdx.x == 0 && t + S < ntile) {
+          const int n0 = own.begin + (t + S) * B;
+          issue_update(L, st, &bars[sidx], s, pcur, n0, min(n0 + B, own.end));
+        }
+      }
+      if (!ok) break;
+      fence_proxy_async_global();
+      if (!(ok = allsum<2>(v2, g, 4))) break;
+      residual = sqrt(v2[0]) / bnorm;
+      n_iter = iter;
+      if (residual < a.tol) break;
+      if (residual != residual && iter < a.max_iter) { nan_fill = true; break; }
+      beta = v2[1] / guard_small(rz);
+      rz = v2[1];
+    }
+    if (nan_fill) {
+      const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+      for (int c = own.begin + (int)threadIdx.x; c < own.end; c += B) x[c] = qnan;
+      residual = qnan;
+      n_iter = a.max_iter;
+    }
+  }
+  if (g.bid == 0 && threadIdx.x == 0) {
+    SolveResult* res = a.ws.result;
+    const int err = ld_volatile_i32(a.ws.err);
+    res->status = err != 0 ? err : (isfinite(residual) ? EAF_OK : EAF_ENONFINITE);
+    res->n_iter = n_iter;
+    res->n_outer = 0;
+    res->sym = 1;
+    res->residual = residual;
+    res->bnorm = bnorm;
+  }
+}
+
+template <int MAXB, int U, int UA>
+__global__ void __launch_bounds__(MAXB, 1) cg_stream_kernel(CgArgs a, int stages) {
+  extern __shared__ __align__(128) double stream_smem[];
+  __shared__ __align__(8) uint64_t bars[kMaxStages];
+  Group g;
+  g.counter = a.ws.counter;
+  g.err = a.ws.err;
+  g.part = a.ws.part;
+  g.stage = group_stage_smem();
+  g.nb = gridDim.x;
+  g.bid = blockIdx.x;
+  g.timeout_ns = a.timeout_ns;
+  g.epoch = 0;
+  if (*a.s.asym != 0) {
+    cg_body<false, U, UA, false>(a, g);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < stages; ++k) mbar_init(&bars[k], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  cg_stream_body(a, g, stream_smem, bars, stream_layout(blockDim.x, a.d.nr, stages));
 }
 
 __global__ void fill_marker_kernel(double* p, int n) {
@@ -800,6 +1158,65 @@ cudaError_t launch_cg_f64_cluster(const MeshDims& d, const SysF64& s, const Grou
     e = cudaLaunchKernelExC(&cfg, k, args);
   }
   return e;
+}
+
+static const void* cg_stream_kernel_ptr(int block) {
+  if (block <= 256) return (const void*)cg_stream_kernel<256, 4, 4>;
+  if (block <= 512) return (const void*)cg_stream_kernel<512, 4, 2>;
+  return (const void*)cg_stream_kernel<1024, 2, 1>;
+}
+
+// Stages of the streaming kernel for blocks of `block` threads on a mesh with
+// nr cells per r row (0 if fewer than two fit in shared memory).
+int stream_stages(int block, int nr) {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+      cudaSuccess)
+    return 0;
+  const long long stage = (long long)stream_layout(block, nr, 2).stage * 8;
+  const long long avail = (long long)optin - 16 * 1024;  // static shared memory and slack
+  long long S = avail / stage;
+  if (S > kMaxStages) S = kMaxStages;
+  return S >= 2 ? (int)S : 0;
+}
+
+int stream_max_coresident(int block, int nr, int sms) {
+  const int S = stream_stages(block, nr);
+  if (S < 2) return 0;
+  const void* k = cg_stream_kernel_ptr(block);
+  const size_t smem = (size_t)stream_layout(block, nr, S).stage * 8 * S;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem) != cudaSuccess)
+    return 0;
+  return per_sm * sms;
+}
+
+cudaError_t launch_cg_f64_stream(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                                 int max_iter, double tol, uint64_t timeout_ns, int grid,
+                                 int block, cudaStream_t st) {
+  const int S = stream_stages(block, d.nr);
+  if (S < 2 || block % 32 != 0) return cudaErrorInvalidValue;
+  CgArgs a;
+  a.d = d;
+  a.s = s;
+  a.ws = ws;
+  a.max_iter = max_iter;
+  a.tol = tol;
+  a.timeout_ns = timeout_ns;
+  const void* k = cg_stream_kernel_ptr(block);
+  const size_t smem = (size_t)stream_layout(block, d.nr, S).stage * 8 * S;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  int stages = S;
+  void* args[] = {&a, &stages};
+  return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(block), args, smem, st);
 }
 
 bool l2_prefetch_pays(long long n) { return (double)n * 128.0 > 96.0e6; }

@@ -83,6 +83,16 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
 // same bits for one launch shape.
 bool l2_prefetch_pays(long long n);
 const void* cg_f64_kernel_ptr(int block, long long n);
+// The same solver with each phase's operands staged in shared memory by
+// bulk copies a few tiles ahead (symmetric operators; the 7-array form runs
+// per-thread loads in the same kernel); bit-identical to cg_f64_kernel on
+// the same launch. Blocks a multiple of 32 threads; stream_stages() says
+// how many tiles are in flight (0: the mesh's rows are too long for it).
+cudaError_t launch_cg_f64_stream(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                                 int max_iter, double tol, uint64_t timeout_ns, int grid,
+                                 int block, cudaStream_t st);
+int stream_stages(int block, int nr);
+int stream_max_coresident(int block, int nr, int sms);
 // The same solver on a grid of thread-block clusters of `cluster` blocks
 // (2..16; grid a multiple of it, at most 128 clusters): its all-reduces fold
 // through the leader block's shared memory in each cluster and a global
@@ -109,12 +119,13 @@ int dsm_max_cells(int cluster);
 // blocks per thread-block cluster (1 = none).
 struct SolverLaunch {
   int grid, block, cluster;
+  int stream = 0;  // 1: the bulk-copy streaming kernel (flat grids only)
 };
 // The launch a handle with the requested shape (0 = automatic) uses on an
 // nr x nth x nz mesh (api.cu): the tuned shape, else the fallback rules,
 // with the cluster size and grid clamped to what the device can run.
 SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int req_grid,
-                           int req_cluster, int form, bool f64);
+                           int req_cluster, int form, bool f64, int req_kernel = 0);
 // Whether the plain FP64 solve on launch L runs the cluster-resident kernel.
 bool runs_resident(const SolverLaunch& L, long long n, bool allowed);
 // Enqueues the plain FP64 solver (reference form) on launch L: the flat,
@@ -134,10 +145,12 @@ const void* cg1_f64_kernel_ptr(int block);
 
 
 // Mixed precision (cg_mixed.cu).
+// `trace` (nullable, 3 * max_outer doubles) receives per refinement step the
+// inner iterations, the inner CG's residual reduction and the outer residual.
 cudaError_t launch_cg_mixed(const MeshDims& d, const SysF64& s, const SysF32& f,
                             const GroupWs& ws, int max_outer, int max_inner,
                             double tol, double inner_tol, uint64_t timeout_ns,
-                            int grid, int block, cudaStream_t st);
+                            int grid, int block, cudaStream_t st, double* trace = nullptr);
 const void* cg_mixed_kernel_ptr();
 
 // ---------------------------------------------------------------------------

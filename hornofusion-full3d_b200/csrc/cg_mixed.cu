@@ -38,6 +38,7 @@ struct MixArgs {
   int max_outer, max_inner;
   double tol, inner_tol;
   uint64_t timeout_ns;
+  double* trace;  // per refinement step: inner iterations, inner reduction, residual
 };
 
 template <bool SYM>
@@ -101,6 +102,8 @@ __device__ void mixed_body(const MixArgs& a, Group& g) {
       if (!(ok = group_allsum<2>(w32, g, 2))) break;
       float rz = w32[1];
       const float seg_start = sqrtf(w32[0]);
+      const int it_before = total_it;
+      float seg_end = seg_start;
       const float stop_abs = fmaxf((float)a.inner_tol * seg_start, (float)(a.tol * bnorm));
       float beta = 0.f;
       // Inner FP32 Jacobi-PCG, two group reductions per iteration (the
@@ -144,6 +147,7 @@ __device__ void mixed_body(const MixArgs& a, Group& g) {
         if (!(ok = group_allsum<2>(v2, g, 5))) break;
         ++total_it;
         const float est = sqrtf(v2[0]);
+        seg_end = est;
         if (!(est >= stop_abs)) break;  // reduced enough (or NaN)
         beta = v2[1] / guard_small(rz);
         rz = v2[1];
@@ -162,6 +166,12 @@ __device__ void mixed_body(const MixArgs& a, Group& g) {
       if (!(ok = group_allsum<1>(w64, g, 0))) break;
       ++outer;
       residual = sqrt(w64[0]) / bnorm;
+      if (a.trace && g.bid == 0 && threadIdx.x == 0) {
+        double* t = a.trace + 3 * (size_t)(outer - 1);
+        t[0] = (double)(total_it - it_before);
+        t[1] = seg_start > 0.f ? (double)seg_end / (double)seg_start : 0.0;
+        t[2] = residual;
+      }
     }
   }
 #undef EAF_OWN_CELLS
@@ -228,6 +238,7 @@ __global__ void __launch_bounds__(kMaxBlock) batch_mixed_kernel(BatchMixArgs a) 
     ma.tol = a.tol;
     ma.inner_tol = a.inner_tol;
     ma.timeout_ns = a.timeout_ns;
+    ma.trace = nullptr;
     if (*bs.s.asym == 0)
       mixed_body<true>(ma, g);
     else
@@ -265,7 +276,7 @@ const void* batch_mixed_kernel_ptr() { return (const void*)batch_mixed_kernel; }
 cudaError_t launch_cg_mixed(const MeshDims& d, const SysF64& s, const SysF32& f,
                             const GroupWs& ws, int max_outer, int max_inner,
                             double tol, double inner_tol, uint64_t timeout_ns,
-                            int grid, int block, cudaStream_t st) {
+                            int grid, int block, cudaStream_t st, double* trace) {
   MixArgs a;
   a.d = d;
   a.s = s;
@@ -276,6 +287,7 @@ cudaError_t launch_cg_mixed(const MeshDims& d, const SysF64& s, const SysF32& f,
   a.tol = tol;
   a.inner_tol = inner_tol;
   a.timeout_ns = timeout_ns;
+  a.trace = trace;
   cudaError_t err = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
   if (err == cudaSuccess) err = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
   if (err != cudaSuccess) return err;

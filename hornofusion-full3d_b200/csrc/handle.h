@@ -24,6 +24,10 @@ struct eaf_cg {
   int block, grid;     // 0 = automatic
   int cluster;         // blocks per thread-block cluster; 0 = automatic, 1 = none
   int resident;        // one-cluster launches keep the system in shared memory
+  int kernel;          // EAF_CG_KERNEL_*: per-thread loads or bulk-copy streaming
+  int last_stream;     // the last FP64 solve ran the streaming kernel
+  double* trace_d;     // mixed form: per refinement step trace (lazy)
+  int trace_cap;       // refinement steps trace_d holds
   int sms;
   uint64_t timeout_ns;
   cudaEvent_t ev[6];   // e2e0, solve0, kern0, kern1, solve1, e2e1

@@ -26,17 +26,17 @@ inline int tuned_lane_width(int nr, int nth, int nz) {
 }
 
 struct TunedLaunch {
-  int nr, nth, nz, block, grid, cluster;
+  int nr, nth, nz, block, grid, cluster, stream;
 };
 
-// (block, grid, blocks per cluster; 1 = no clusters) of the single-system
-// persistent solver.
+// (block, grid, blocks per cluster (1 = no clusters), bulk-copy streaming
+// kernel (1) or per-thread loads (0)) of the single-system persistent solver.
 static constexpr TunedLaunch kTunedLaunches[] = {
-    {12, 24, 16, 288, 16, 16},
-    {18, 36, 24, 512, 16, 16},
-    {35, 70, 50, 256, 148, 1},
-    {60, 120, 84, 512, 148, 1},
-    {120, 240, 168, 1024, 148, 1},
+    {12, 24, 16, 288, 16, 16, 0},
+    {18, 36, 24, 512, 16, 16, 0},
+    {35, 70, 50, 256, 148, 1, 0},
+    {60, 120, 84, 512, 148, 1, 0},
+    {120, 240, 168, 1024, 148, 1, 0},
 };
 
 // Most blocks a tuned launch of a mesh of at most `max_cells` cells can run
@@ -51,12 +51,13 @@ constexpr int max_tuned_grid_up_to(long long max_cells) {
 }
 
 inline bool tuned_single_launch(int nr, int nth, int nz, int* block, int* grid,
-                                int* cluster = nullptr) {
+                                int* cluster = nullptr, int* stream = nullptr) {
   for (const TunedLaunch& t : kTunedLaunches)
     if (t.nr == nr && t.nth == nth && t.nz == nz) {
       *block = t.block;
       *grid = t.grid;
       if (cluster) *cluster = t.cluster;
+      if (stream) *stream = t.stream;
       return true;
     }
   return false;

@@ -119,6 +119,13 @@ int eaf_cg_solve_mixed_device(eaf_cg_t h, const double* aW, const double* aE,
                               double inner_tol, double* residual, int* n_iter,
                               int* n_outer);
 
+/* Trace of the last mixed-precision solve: for each refinement step (at most
+ * max_steps), three doubles -- the inner FP32 iterations of the step, the
+ * reduction of the inner CG's recurred residual over the step, and the FP64
+ * outer residual ||Su - A phi|| / ||Su|| after it. n_steps receives the
+ * number of steps copied. No reference counterpart (diagnostics). */
+int eaf_cg_mixed_trace(eaf_cg_t h, double* steps, int max_steps, int* n_steps);
+
 /* Launch shape of the persistent kernel: threads per block and number of
  * co-resident blocks (0 = automatic). Used by the autotuner. */
 int eaf_cg_set_launch(eaf_cg_t h, int block_threads, int grid_blocks);
@@ -149,6 +156,18 @@ int eaf_cg_last_cluster(eaf_cg_t h, int* cluster_blocks);
  * touches no global memory. It gives the same bits as the global-memory
  * cluster kernel on that launch (resident = 0). No reference counterpart. */
 int eaf_cg_set_resident(eaf_cg_t h, int resident);
+
+/* Kernel of the plain FP64 solve on a flat (cluster-free) grid: per-thread
+ * loads (EAF_CG_KERNEL_LOADS), or each phase's operands staged in shared
+ * memory by bulk copies a few tiles ahead of use (EAF_CG_KERNEL_STREAM),
+ * or the tuned choice of the mesh (EAF_CG_KERNEL_AUTO). Both give the same
+ * bits on the same launch shape. eaf_cg_last_kernel reports which ran. No
+ * reference counterpart. */
+#define EAF_CG_KERNEL_AUTO 0
+#define EAF_CG_KERNEL_LOADS 1
+#define EAF_CG_KERNEL_STREAM 2
+int eaf_cg_set_kernel(eaf_cg_t h, int kernel);
+int eaf_cg_last_kernel(eaf_cg_t h, int* kernel);
 
 /* Line-by-line TDMA on the handle's mesh: replaces tdma_3d_mpi
  * (src/mod_solver_3d.f90:252-366, serial branch; callers in momentum,

@@ -96,3 +96,25 @@ def test_mixed_rejects_bad_inner_tolerance():
     s = g.make_system(*g.SMOKE, seed=0)
     with pytest.raises(eaf.EafError):
         mixed(s, g.zeros_phi(12, 24, 16), 1e-8, inner_tol=1.5)
+
+
+def test_mixed_trace_records_every_refinement_step():
+    """The per-step trace: one entry per refinement step, inner iterations
+    summing to the reported total, the last outer residual equal to the
+    returned one, and each step but the last reaching its inner reduction
+    (inner_tol, compared in FP32) unless capped."""
+    eaf = pkg()
+    g = gen()
+    s = g.make_system(12, 24, 16, 8, seed=1)
+    phi = g.zeros_phi(12, 24, 16)
+    with eaf.CGSolver(12, 24, 16) as cg:
+        res, nit, nout, st = cg.solve_mixed(s.arrays(), phi, tol=1e-10, inner_tol=0.1,
+                                            max_outer=60, max_inner=4000)
+        trace = cg.mixed_trace()
+        assert len(trace) == nout and st == 0
+        assert sum(t["inner_iterations"] for t in trace) == nit
+        assert trace[-1]["residual"] == res
+        assert all(t["inner_reduction"] <= 0.1 * (1 + 1e-6) or t["inner_iterations"] == 4000
+                   for t in trace[:-1])
+        cg.solve(s.arrays(), g.zeros_phi(12, 24, 16), 100, 1e-8)
+        assert cg.mixed_trace() == []
