@@ -787,69 +787,107 @@ def run_pstep(args):
 def run_batch(args):
     """96 uneven systems (40 at 12x24x16, 30 at 18x36x24, 20 at 35x70x50,
     6 at 60x120x84; seed = system id) in one persistent launch replayed from
-    a CUDA graph, against the same systems solved one by one."""
+    a CUDA graph, against the same systems solved one by one.
+
+    Under torchrun (N ranks, one GPU each) the systems are partitioned
+    across the ranks by estimated work within each GPU's HBM budget
+    (multigpu.partition), every rank solves its share in one batched launch
+    of its own, and the line reports the whole job: all systems over the
+    slowest rank's device time (strong scaling: the mix is fixed)."""
     import torch
     eaf = importlib.import_module(PKG)
     g = importlib.import_module(PKG + ".eafgen")
-    systems = []
+    mg = importlib.import_module(PKG + ".multigpu")
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    specs = []
     for (dims, count) in g.BATCH_MIX:
         for _ in range(count):
-            systems.append(g.make_system(*dims, seed=len(systems)))
-    dims = [(s.nr, s.nth, s.nz) for s in systems]
-    dev = [[torch.from_numpy(a).cuda() for a in s.arrays()] for s in systems]
-    phis = [torch.zeros(g.halo_shape(*d), dtype=torch.float64, device="cuda") for d in dims]
-    total_cells = sum(a * b * c for a, b, c in dims)
-    out = {}
-    with eaf.Batch(dims) as b:
-        for i in range(len(systems)):
-            b.set_system(i, dev[i][:8], phis[i], device_ptrs=True)
-        grid, block, nlanes = b.plan()
-        for form in ("fp64", "mixed"):
-            mixed = form == "mixed"
+            specs.append(dims)
+    items = [mg.Item(k, d[0] * d[1] * d[2], mg.device_footprint(*d[:3]),
+                     mg.estimated_work(*d[:3])) for k, d in enumerate(specs)]
+    plans = {}
+
+    def share(form):
+        mixed = form == "mixed"
+
+        def solve_share(mine):
+            keys = [it.key for it in mine]
+            if not keys:
+                return 0.0, {}
+            systems = [g.make_system(*specs[k], seed=k) for k in keys]
+            dims = [(s.nr, s.nth, s.nz) for s in systems]
+            dev = [[torch.from_numpy(a).cuda() for a in s.arrays()] for s in systems]
+            phis = [torch.zeros(g.halo_shape(*d), dtype=torch.float64, device="cuda")
+                    for d in dims]
             kw = dict(mixed=mixed, max_iter=args.mixed_inner if mixed else MAX_ITER,
                       tol=TOL, max_outer=args.mixed_outer, inner_tol=0.1)
-            for _ in range(args.warmup if not mixed else 1):
-                for p in phis:
-                    p.zero_()
-                b.solve(**kw)
-            ms, ci, worst = 0.0, 0, 0.0
-            steps = args.steps if not mixed else 1
-            for _ in range(steps):
-                for p in phis:
-                    p.zero_()
-                torch.cuda.synchronize()
-                b.solve(**kw)
-                ms += b.last_ms
+            with eaf.Batch(dims) as b:
                 for i in range(len(systems)):
+                    b.set_system(i, dev[i][:8], phis[i], device_ptrs=True)
+                plans[form] = b.plan()
+                plans["widths"] = sorted({(d, b.lane_width(i)) for i, d in enumerate(dims)})
+                for _ in range(args.warmup if not mixed else 1):
+                    for p in phis:
+                        p.zero_()
+                    b.solve(**kw)
+                ms = 0.0
+                steps = args.steps if not mixed else 1
+                for _ in range(steps):
+                    for p in phis:
+                        p.zero_()
+                    torch.cuda.synchronize()
+                    b.solve(**kw)
+                    ms += b.last_ms
+                res = {}
+                for i, k in enumerate(keys):
                     r, nit, no, st = b.result(i)
-                    ci += (dims[i][0] * dims[i][1] * dims[i][2]) * nit
-                    worst = max(worst, r)
-            out[form] = {"ms_per_batch": ms / steps, "cell_iters_per_s": ci / (ms / 1e3),
-                         "solves_per_s": len(systems) * steps / (ms / 1e3),
-                         "max_residual": worst}
-        widths = sorted({(d, b.lane_width(i)) for i, d in enumerate(dims)})
-    # the same systems one by one through the single-system FP64 solver
-    seq_ms = 0.0
-    for i, s in enumerate(systems):
-        with eaf.CGSolver(*dims[i]) as cg:
-            phis[i].zero_()
-            cg.solve(dev[i][:8], phis[i], MAX_ITER, TOL, device_ptrs=True)
-            phis[i].zero_()
-            torch.cuda.synchronize()
-            cg.solve(dev[i][:8], phis[i], MAX_ITER, TOL, device_ptrs=True)
-            seq_ms += cg.last_timing()["solve_ms"]
-    seq = {"ms_per_96": seq_ms, "solves_per_s": len(systems) / (seq_ms / 1e3)}
+                    res[k] = (r, nit, st)
+            return ms / steps / 1e3, res
+        return solve_share
+
+    out = {}
+    for form in ("fp64", "mixed"):
+        t, res, parts = mg.solve_sharded(items, share(form))
+        ci = sum(specs[k][0] * specs[k][1] * specs[k][2] * res[k][1] for k in res)
+        out[form] = {"ms_per_batch": t * 1e3, "cell_iters_per_s": ci / t,
+                     "solves_per_s": len(specs) / t,
+                     "max_residual": max(r for r, _, _ in res.values()),
+                     "systems_per_rank": [len(p) for p in parts]}
+    seq = None
+    if world == 1:
+        # the same systems one by one through the single-system FP64 solver
+        seq_ms = 0.0
+        for k, d in enumerate(specs):
+            s = g.make_system(*d, seed=k)
+            dev = [torch.from_numpy(a).cuda() for a in s.arrays()]
+            phi = torch.zeros(g.halo_shape(*d[:3]), dtype=torch.float64, device="cuda")
+            with eaf.CGSolver(*d[:3]) as cg:
+                cg.solve(dev[:8], phi, MAX_ITER, TOL, device_ptrs=True)
+                phi.zero_()
+                torch.cuda.synchronize()
+                cg.solve(dev[:8], phi, MAX_ITER, TOL, device_ptrs=True)
+                seq_ms += cg.last_timing()["solve_ms"]
+        seq = {"ms_per_96": seq_ms, "solves_per_s": len(specs) / (seq_ms / 1e3)}
+    if rank != 0:
+        return 0
+    total_cells = sum(d[0] * d[1] * d[2] for d in specs)
+    grid, block, nlanes = plans.get("fp64", (0, 0, 0))
     line = _base_line("batched pressure-CG solves/s (96-system mix, one launch)",
                       out["fp64"]["solves_per_s"], "solves/s", args.steps, args.warmup,
                       out["fp64"]["ms_per_batch"], "96 uneven systems, one persistent launch",
-                      {"systems": len(systems), "cells": total_cells,
+                      {"systems": len(specs), "cells": total_cells,
                        "mix": [[list(d[:3]), c] for d, c in g.BATCH_MIX],
-                       "plan": {"grid": grid, "block": block, "lanes": nlanes},
-                       "lane_widths": [[list(d), w] for d, w in widths],
-                       "graph": "pack + persistent batch kernel + unpack captured once, replayed"})
+                       "plan_rank0": {"grid": grid, "block": block, "lanes": nlanes},
+                       "lane_widths": [[list(d), w] for d, w in plans.get("widths", [])],
+                       "graph": "pack + persistent batch kernel + unpack captured once, replayed",
+                       "parallelism": f"systems sharded over {world} GPU(s), one batch each"})
+    line["n_gpus"] = world
+    line["scaling"] = "strong"
     line["forms"] = out
-    line["sequential_fp64"] = seq
-    line["speedup_vs_sequential_fp64"] = out["fp64"]["solves_per_s"] / seq["solves_per_s"]
+    if seq is not None:
+        line["sequential_fp64"] = seq
+        line["speedup_vs_sequential_fp64"] = out["fp64"]["solves_per_s"] / seq["solves_per_s"]
     print(json.dumps(line), flush=True)
     return 0
 
@@ -984,6 +1022,23 @@ def run_fixed(args):
     return 0
 
 
+def run_sharded_workload(fn, args):
+    """A workload whose independent systems are sharded over the ranks of a
+    torchrun launch (one GPU each, NCCL for the host-side result gather)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    local_rank = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local_rank)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device(f"cuda:{local_rank}"))
+    try:
+        return fn(args)
+    finally:
+        dist.destroy_process_group()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1018,6 +1073,8 @@ def main(argv=None):
     ap.add_argument("--batch-size", type=int, default=0)
     ap.add_argument("--fixed-tdma", action="store_true")
     args = ap.parse_args(argv)
+    if args.workload == "batch" and args.impl == "ours" and _env_int("WORLD_SIZE", 1) > 1:
+        return run_sharded_workload(run_batch, args)
     if args.workload != "production" and args.impl == "ours":
         return {"fine": run_fine, "batch": run_batch, "serve": run_serve,
                 "tdma": run_tdma, "pcorr": run_pcorr,

@@ -97,3 +97,46 @@ def gather_results(local: dict, group=None) -> dict:
             raise RuntimeError(f"keys solved on two ranks: {sorted(overlap)[:5]}")
         merged.update(p)
     return merged
+
+
+class ShardError(RuntimeError):
+    """A rank's share failed; raised on every rank of the collective."""
+
+
+def solve_sharded(items: list[Item], solve_share, group=None,
+                  budget: float | None = None) -> tuple[float, dict, list[list[Item]]]:
+    """Collective over `group` (or a single process when torch.distributed is
+    not initialised): partition `items` across the ranks (`partition`), call
+    `solve_share(my_items) -> (elapsed_s, {key: result})` on every rank with
+    its share, and return (the slowest rank's elapsed seconds, the results
+    of every rank merged by key, the partition) on every rank.
+
+    Every rank takes exactly one collective step (an object all-gather of
+    its error, time and results), also when its solve raised, so a failure
+    on one rank cannot leave the others waiting: every rank then raises
+    ShardError naming the failed ranks."""
+    import torch.distributed as dist
+    on = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size(group) if on else 1
+    rank = dist.get_rank(group) if on else 0
+    parts = partition(items, world, budget)
+    err, elapsed, local = None, 0.0, {}
+    try:
+        elapsed, local = solve_share(parts[rank])
+    except Exception as exc:  # reported to every rank below
+        err = f"{type(exc).__name__}: {exc}"
+    if on:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (err, float(elapsed), local), group=group)
+    else:
+        gathered = [(err, float(elapsed), local)]
+    failed = [(r, e) for r, (e, _, _) in enumerate(gathered) if e is not None]
+    if failed:
+        raise ShardError("; ".join(f"rank {r}: {e}" for r, e in failed))
+    merged: dict = {}
+    for _, _, p in gathered:
+        overlap = set(merged) & set(p)
+        if overlap:
+            raise RuntimeError(f"keys solved on two ranks: {sorted(overlap)[:5]}")
+        merged.update(p)
+    return max(t for _, t, _ in gathered), merged, parts

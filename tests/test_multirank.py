@@ -113,3 +113,84 @@ def test_two_ranks_gloo_match_single_process(tmp_path):
         total_units += d[0] * d[1] * d[2] * nit
     assert got["units"] == total_units
     assert got["tmax"] >= got["el"]
+
+
+def _oracle_share(mine):
+    """The CPU stand-in for one rank's batched GPU solve of its share."""
+    import time
+
+    import oracle
+    from conftest import gen as _gen
+    g = _gen()
+    t0 = time.perf_counter()
+    out = {}
+    for it in mine:
+        d = MIX[it.key]
+        s = g.make_system(*d, seed=it.key)
+        phi = g.zeros_phi(*d[:3])
+        res, nit = oracle.cg(s, phi, 10000, 1e-8)
+        out[it.key] = (res, nit, float(g.interior(phi).sum()))
+    return time.perf_counter() - t0, out
+
+
+def _failing_share(mine):
+    import torch.distributed as dist
+    if dist.get_rank() == 1:
+        raise RuntimeError("device lost")
+    return _oracle_share(mine)
+
+
+def _sharded_worker(rank, world, port, out_dir, fail):
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import datetime
+    import json
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        m = mg()
+        try:
+            t, merged, parts = m.solve_sharded(items(), _failing_share if fail else _oracle_share)
+            outcome = {"t": t, "merged": {str(k): v for k, v in merged.items()},
+                       "parts": [[i.key for i in p] for p in parts]}
+        except m.ShardError as exc:
+            outcome = {"error": str(exc)}
+        dist.barrier()  # the group still works after a failed share
+        with open(os.path.join(out_dir, f"out{rank}.json"), "w") as f:
+            json.dump(outcome, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_solve_sharded_two_ranks_equals_single_process(tmp_path):
+    """The batch path's sharding driver (multigpu.solve_sharded) on two gloo
+    ranks, with the oracle standing in for each rank's GPU batch: every rank
+    gets the complete merged results, equal to the single-process run, and
+    the slowest rank's time."""
+    import json
+
+    import torch.multiprocessing as mp
+    mp.start_processes(_sharded_worker, args=(2, _free_port(), str(tmp_path), False),
+                       nprocs=2, join=True, start_method="spawn")
+    outs = [json.load(open(tmp_path / f"out{r}.json")) for r in range(2)]
+    assert outs[0]["merged"] == outs[1]["merged"] and outs[0]["t"] == outs[1]["t"]
+    assert sorted(k for p in outs[0]["parts"] for k in p) == list(range(len(MIX)))
+    assert all(len(p) > 0 for p in outs[0]["parts"])
+    _, single = _oracle_share(items())
+    assert outs[0]["merged"] == {str(k): list(v) for k, v in single.items()}
+
+
+def test_solve_sharded_failure_on_one_rank_raises_everywhere(tmp_path):
+    import json
+
+    import torch.multiprocessing as mp
+    mp.start_processes(_sharded_worker, args=(2, _free_port(), str(tmp_path), True),
+                       nprocs=2, join=True, start_method="spawn")
+    for r in range(2):
+        out = json.load(open(tmp_path / f"out{r}.json"))
+        assert out == {"error": "rank 1: RuntimeError: device lost"}
