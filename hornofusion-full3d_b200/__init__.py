@@ -270,11 +270,17 @@ class CGSolver:
         1 for none, 0 for the tuned choice of the mesh."""
         check(self._lib.eaf_cg_set_cluster(self._h, int(cluster)), "set_cluster")
 
-    def set_resident(self, resident: bool = True) -> None:
+    RESIDENT_OFF = 0
+    RESIDENT_MBARRIER = 1
+    RESIDENT_CLUSTER_BARRIER = 2
+
+    def set_resident(self, mode: int = 1) -> None:
         """One-cluster launches of a mesh that fits keep the system in the
-        cluster's shared memory (default) or run the global-memory cluster
-        kernel; both give the same bits."""
-        check(self._lib.eaf_cg_set_resident(self._h, int(bool(resident))), "set_resident")
+        cluster's shared memory, the blocks signalling their partials by
+        mbarrier arrivals (RESIDENT_MBARRIER, default) or a cluster barrier
+        (RESIDENT_CLUSTER_BARRIER), or run the global-memory cluster kernel
+        (RESIDENT_OFF); all give the same bits."""
+        check(self._lib.eaf_cg_set_resident(self._h, int(mode)), "set_resident")
 
     def mixed_trace(self, max_steps: int = 1000) -> list:
         """Per refinement step of the last mixed-precision solve: inner FP32
@@ -381,6 +387,16 @@ class Batch:
         check(self._lib.eaf_batch_plan(self._h, ctypes.byref(g), ctypes.byref(b),
                                        ctypes.byref(n)), "eaf_batch_plan")
         return g.value, b.value, n.value
+
+    def system_plan(self, sys: int) -> tuple:
+        """The oracle plan of a system's FP64 dots: (lane width, 512) for a
+        system on a lane, or the single-system launch (grid, block[, cluster])
+        of a large system solved over the whole GPU after the batched launch."""
+        g, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._lib.eaf_batch_system_plan(self._h, int(sys), ctypes.byref(g),
+                                              ctypes.byref(b), ctypes.byref(c)),
+              "eaf_batch_system_plan")
+        return (g.value, b.value) if c.value <= 1 else (g.value, b.value, c.value)
 
     def set_system(self, sys: int, arrays, phi, device_ptrs: bool = False) -> None:
         arrays = list(arrays)

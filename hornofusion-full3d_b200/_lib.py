@@ -148,6 +148,7 @@ SIGNATURES = [
     ("eaf_batch_set_width", _ci, [_vp, _ci, _ci]),
     ("eaf_batch_lane_width", _ci, [_vp, _ci, _pi]),
     ("eaf_batch_plan", _ci, [_vp, _pi, _pi, _pi]),
+    ("eaf_batch_system_plan", _ci, [_vp, _ci, _pi, _pi, _pi]),
     ("eaf_batch_set_system", _ci, [_vp, _ci] + [_vp] * 9),
     ("eaf_batch_set_system_device", _ci, [_vp, _ci] + [_vp] * 9),
     ("eaf_batch_solve", _ci, [_vp, _ci, _ci, _cd, _ci, _cd]),

@@ -172,11 +172,13 @@ bool runs_resident(const SolverLaunch& L, long long n, bool allowed) {
   return allowed && L.cluster > 1 && L.grid == L.cluster && n <= dsm_max_cells(L.cluster);
 }
 
-cudaError_t launch_f64_solver(const SolverLaunch& L, bool resident, const MeshDims& d,
+cudaError_t launch_f64_solver(const SolverLaunch& L, int resident, const MeshDims& d,
                               const SysF64& s, const GroupWs& ws, size_t slot_doubles,
                               int max_iter, double tol, uint64_t timeout_ns, cudaStream_t st) {
-  if (runs_resident(L, d.n, resident))
-    return launch_cg_f64_dsm(d, s, ws, max_iter, tol, L.block, L.cluster, st);
+  if (runs_resident(L, d.n, resident != 0))
+    return launch_cg_f64_dsm(d, s, ws, max_iter, tol, L.block, L.cluster, st,
+                             resident == 2 ? kDsmSignalClusterBarrier : kDsmSignalMbarrier,
+                             timeout_ns);
   if (L.cluster > 1)
     return launch_cg_f64_cluster(d, s, ws, ws.part, slot_doubles, max_iter, tol, timeout_ns,
                                  L.grid, L.block, L.cluster, st);
@@ -360,7 +362,7 @@ int eaf_cg_last_kernel(eaf_cg_t h, int* kernel) {
 }
 
 int eaf_cg_set_resident(eaf_cg_t h, int resident) {
-  if (!h || (resident != 0 && resident != 1)) return EAF_EINVAL;
+  if (!h || resident < 0 || resident > 2) return EAF_EINVAL;
   h->resident = resident;
   return EAF_OK;
 }
@@ -486,7 +488,7 @@ int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts&
       EAF_CUDA(eaf::launch_cg1_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,
                                    grid, block, h->st));
     else
-      EAF_CUDA(eaf::launch_f64_solver(L, h->resident != 0, h->d, h->s, h->ws,
+      EAF_CUDA(eaf::launch_f64_solver(L, h->resident, h->d, h->s, h->ws,
                                       kPartTableDoubles(h), o.max_iter, o.tol,
                                       h->timeout_ns, h->st));
   }

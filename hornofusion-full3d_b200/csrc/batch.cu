@@ -8,6 +8,17 @@
 // lanes in proportion to its modelled work (longest-processing-time queue
 // assignment inside a class) until the co-resident blocks are used up.
 //
+// Large systems. A system of at least kSoloCells cells (and no explicit
+// width) does not take a lane: after the batched launch, the large systems
+// run one after another, each over the whole GPU with the launch the
+// single-system solver uses for its mesh (tuned table), in the same graph.
+// A lane narrow enough to share the GPU with the small systems runs a
+// system whose working set fills the L2 many times slower than the whole
+// GPU does, and several such lanes side by side no longer fit in L2 at all;
+// one at a time at full width each stays L2-resident. The association of a
+// large system's dot products is that of its single-system launch, so its
+// result is again the same alone and in any mix (eaf_batch_system_plan).
+//
 // Model of one system's solve on w blocks of 512 threads (B200 figures):
 //   iterations   ~ 8 sqrt(cells)              (Jacobi-PCG on these meshes)
 //   per iteration = 2 phases + 2 group reductions
@@ -36,7 +47,8 @@ using eaf::SolveResult;
 
 namespace {
 
-
+constexpr long long kSoloCells = 300000;
+constexpr int kSoloPartSlots = 8;
 
 double model_iter_us(long long cells, int w) {
   const double cpb = (double)cells / w;
@@ -198,6 +210,13 @@ struct eaf_batch {
   unsigned long long* d_counters;
   double* d_parts;
   int* d_err;
+  // large systems solved one after another at full width
+  std::vector<char> solo;
+  std::vector<eaf::SolverLaunch> solo_f64;
+  double* d_solo_part;
+  unsigned long long* d_solo_counter;
+  int* d_solo_err;
+  int sms;
   // graph
   cudaGraphExec_t exec;
   bool graph_valid;
@@ -214,6 +233,8 @@ int width_for(const eaf_batch* b, int s) {
   if (b->width[s] > 0) return b->width[s];
   return eaf::tuned_lane_width(b->nr[s], b->nth[s], b->nz[s]);
 }
+
+bool is_solo(const eaf_batch* b, int s) { return b->width[s] == 0 && b->n[s] >= kSoloCells; }
 
 void free_batch(eaf_batch* b) {
   if (b->graph_valid) cudaGraphExecDestroy(b->exec);
@@ -233,6 +254,9 @@ void free_batch(eaf_batch* b) {
   cudaFree(b->d_counters);
   cudaFree(b->d_parts);
   cudaFree(b->d_err);
+  cudaFree(b->d_solo_part);
+  cudaFree(b->d_solo_counter);
+  cudaFree(b->d_solo_err);
   if (b->h_res) cudaFreeHost(b->h_res);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
@@ -269,11 +293,31 @@ int plan(eaf_batch* b) {
   int G = 0;
   int rc = eaf::batch_capacity(b->device, &G);
   if (rc != EAF_OK) return rc;
-  std::vector<int> widths;
-  for (int s = 0; s < b->nsys; ++s) widths.push_back(width_for(b, s));
+  std::vector<int> widths, ids;
+  std::vector<long long> cells;
+  b->solo.assign(b->nsys, 0);
+  b->solo_f64.assign(b->nsys, eaf::SolverLaunch{0, 0, 1});
+  for (int s = 0; s < b->nsys; ++s) {
+    if (is_solo(b, s)) {
+      b->solo[s] = 1;
+      b->solo_f64[s] = eaf::choose_launch(b->nr[s], b->nth[s], b->nz[s], b->sms, 0, 0, 0,
+                                          EAF_CG_FORM_REFERENCE, true);
+      b->solo_f64[s].stream = 0;  // compact arrays here carry no padding cell
+      continue;
+    }
+    ids.push_back(s);
+    widths.push_back(width_for(b, s));
+    cells.push_back(b->n[s]);
+  }
   eaf::LanePlan lp;
-  rc = eaf::plan_lanes(widths, b->n, G, &lp);
-  if (rc != EAF_OK) return rc;
+  if (!ids.empty()) {
+    rc = eaf::plan_lanes(widths, cells, G, &lp);
+    if (rc != EAF_OK) return rc;
+    for (int& q : lp.queue) q = ids[q];  // lane-system index -> system id
+  } else {
+    G = 0;
+    lp.q_begin.assign(1, 0);
+  }
   b->lane_of_block = lp.lane_of_block;
   b->lane_first = lp.lane_first;
   b->lane_width = lp.lane_width;
@@ -294,8 +338,9 @@ int plan(eaf_batch* b) {
     e = cudaMemcpy(b->d_tab, host.data(), sizeof(int) * host.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMalloc((void**)&b->d_counters,
-                   sizeof(unsigned long long) * eaf::kCounterStride * b->nlanes);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_parts, sizeof(double) * 8 * G);
+                   sizeof(unsigned long long) * eaf::kCounterStride *
+                       (b->nlanes > 0 ? b->nlanes : 1));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_parts, sizeof(double) * 8 * (G > 0 ? G : 1));
   if (e != cudaSuccess) {
     eaf::set_error("eaf_batch: plan tables", e);
     return EAF_ENOMEM;
@@ -321,7 +366,7 @@ cudaError_t enqueue(eaf_batch* b) {
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_err, 0, sizeof(int), b->st);
   // external event-record nodes: the graph's launches can be timed
   if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->ev0, b->st, cudaEventRecordExternal);
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && b->grid > 0) {
     const BatchTables t = tables(b);
     if (b->g_mixed)
       e = eaf::launch_batch_mixed(t, b->grid, eaf::kBatchBlock, b->g_max_outer, b->g_max_iter,
@@ -329,6 +374,22 @@ cudaError_t enqueue(eaf_batch* b) {
     else
       e = eaf::launch_batch_f64(t, b->grid, eaf::kBatchBlock, b->g_max_iter, b->g_tol,
                                 b->timeout_ns, b->st);
+  }
+  // the large systems, one after another over the whole GPU
+  for (int s = 0; s < b->nsys && e == cudaSuccess; ++s) {
+    if (!b->solo[s]) continue;
+    const eaf::GroupWs ws = {b->d_solo_part, b->d_solo_counter, b->d_solo_err, b->d_res + s};
+    if (b->g_mixed) {
+      const eaf::SolverLaunch L = eaf::choose_launch(b->nr[s], b->nth[s], b->nz[s], b->sms, 0,
+                                                     0, 0, EAF_CG_FORM_REFERENCE, false);
+      e = eaf::launch_cg_mixed(b->sys[s].d, b->sys[s].s, b->sys[s].f, ws, b->g_max_outer,
+                               b->g_max_iter, b->g_tol, b->g_inner_tol, b->timeout_ns,
+                               L.grid, L.block, b->st);
+    } else {
+      e = eaf::launch_f64_solver(b->solo_f64[s], 1, b->sys[s].d, b->sys[s].s, ws,
+                                 (size_t)kSoloPartSlots * b->sms * 8, b->g_max_iter,
+                                 b->g_tol, b->timeout_ns, b->st);
+    }
   }
   if (e == cudaSuccess) e = cudaEventRecordWithFlags(b->ev1, b->st, cudaEventRecordExternal);
   for (int s = 0; s < b->nsys && e == cudaSuccess; ++s)
@@ -415,6 +476,12 @@ int eaf_batch_create(eaf_batch_t* out, int nsys, const int* dims, int device) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_sys, sizeof(BatchSys) * nsys);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_res, sizeof(SolveResult) * nsys);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_err, sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&b->d_solo_part, sizeof(double) * kSoloPartSlots * b->sms * 8);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_solo_counter, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_solo_err, sizeof(int));
   if (e == cudaSuccess) e = cudaHostAlloc((void**)&b->h_res, sizeof(SolveResult) * nsys, 0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
@@ -452,6 +519,23 @@ int eaf_batch_set_width(eaf_batch_t b, int sys, int width) {
 int eaf_batch_lane_width(eaf_batch_t b, int sys, int* width) {
   if (!b || !width || sys < 0 || sys >= b->nsys) return EAF_EINVAL;
   *width = width_for(b, sys);
+  return EAF_OK;
+}
+
+int eaf_batch_system_plan(eaf_batch_t b, int sys, int* grid, int* block, int* cluster) {
+  if (!b || !grid || !block || !cluster || sys < 0 || sys >= b->nsys) return EAF_EINVAL;
+  eaf::DeviceGuard guard(b->device);
+  const int rc = plan(b);
+  if (rc != EAF_OK) return rc;
+  if (b->solo[sys]) {
+    *grid = b->solo_f64[sys].grid;
+    *block = b->solo_f64[sys].block;
+    *cluster = b->solo_f64[sys].cluster;
+  } else {
+    *grid = width_for(b, sys);
+    *block = eaf::kBatchBlock;
+    *cluster = 1;
+  }
   return EAF_OK;
 }
 

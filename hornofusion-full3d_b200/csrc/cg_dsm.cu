@@ -14,12 +14,15 @@
 //     double-buffered direction in its shared memory; a neighbour cell that
 //     another block owns is read from that block's shared memory
 //     (ld.shared::cluster);
-//   * an all-reduce is one cluster barrier: every block writes its partial
-//     into every block's shared memory, and after the barrier every thread
+//   * an all-reduce is one exchange: every block writes its partial into
+//     every block's shared memory and signals it, and then every thread
 //     folds the C partials in rank order. The association is that of the
 //     cluster all-reduce with one cluster (the oracle's plan (C, B, C)), so
 //     the solve is bit-identical to cg_cluster_kernel on the same launch
-//     shape and to the oracle.
+//     shape and to the oracle. The signal is either a remote arrival on an
+//     mbarrier of each block (release at cluster scope, one arrival per
+//     block and phase, barriers double-buffered by all-reduce parity; the
+//     default) or a full cluster barrier.
 //
 // Global memory is read once (the packed system) and written once (x and
 // the result). There is no global synchronisation and no wait that another
@@ -43,9 +46,10 @@ enum { kAP, kAW, kAE, kAS, kAN, kAB, kAT, kX, kR, kZ, kP0, kP1, kQ };
 struct DsmArgs {
   MeshDims d;
   SysF64 s;      // the packed compact system (read) and x (written back)
-  GroupWs ws;    // result
+  GroupWs ws;    // result and error word
   int max_iter;
   double tol;
+  uint64_t timeout_ns;
   int chunk;     // cells per block
   FastDiv fd_chunk;
 };
@@ -53,7 +57,33 @@ struct DsmArgs {
 struct PartSmem {
   double part[2][kMaxClusterSize][kClusterSlotsNV];  // by parity, by rank
   double warp[kClusterSlotsNV][32];
+  uint64_t bar[2];  // arrivals of the C blocks' partials, by parity
 };
+
+// Signalling of the exchange: mbarrier arrivals (MB) or a cluster barrier.
+struct Exchange {
+  int C, rank, parity;
+  uint32_t phase;  // completion parity expected next, bit per barrier
+  int* err;
+  uint64_t timeout_ns;
+};
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(
+                   cluster_addr)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test_cluster(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 
 __device__ __forceinline__ double ld_cluster_f64(uint32_t a) {
   double v;
@@ -77,11 +107,12 @@ struct Dsm {
   }
 };
 
-// One cluster barrier: every block's partials go to every block, then each
-// thread folds them in rank order (starting from rank 0's).
-template <int NV>
-__device__ __forceinline__ void dsm_allsum(double (&v)[NV], PartSmem& ps, int C, int rank,
-                                           int parity) {
+// Every block's partials go to every block, then each thread folds them in
+// rank order (starting from rank 0's). Returns false if a bounded wait gave
+// up (then every thread of the block returns false).
+template <int NV, bool MB>
+__device__ __forceinline__ bool dsm_allsum(double (&v)[NV], PartSmem& ps, Exchange& x) {
+  const int C = x.C, rank = x.rank, parity = x.parity;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nthreads = blockDim.x;
 #pragma unroll
@@ -106,16 +137,42 @@ __device__ __forceinline__ void dsm_allsum(double (&v)[NV], PartSmem& ps, int C,
       const uint32_t dst = cluster_map(smem_addr(&ps.part[parity][rank][0]), (uint32_t)lane);
 #pragma unroll
       for (int m = 0; m < NV; ++m) st_cluster_f64(dst + 8u * m, blk[m]);
+      if (MB) mbar_arrive_remote(cluster_map(smem_addr(&ps.bar[parity]), (uint32_t)lane));
     }
     __syncwarp();
   }
-  cluster_sync_all();
+  bool ok = true;
+  if (MB) {
+    // Every thread acquires the C arrivals itself (bounded wait).
+    const uint32_t a = smem_addr(&ps.bar[parity]);
+    const uint32_t want = (x.phase >> parity) & 1u;
+    if (!mbar_test_cluster(a, want)) {
+      const uint64_t t0 = global_ns();
+      uint32_t spins = 0;
+      while (!mbar_test_cluster(a, want)) {
+        if ((++spins & 255u) == 0) {
+          if (ld_volatile_i32(x.err) != 0) { ok = false; break; }
+          if (global_ns() - t0 > x.timeout_ns) {
+            atomicCAS(x.err, 0, (int)EAF_ETIMEOUT);
+            ok = false;
+            break;
+          }
+        }
+      }
+    }
+    x.phase ^= 1u << parity;
+    ok = __syncthreads_and(ok) != 0;
+  } else {
+    cluster_sync_all();
+  }
+  x.parity ^= 1;
 #pragma unroll
   for (int m = 0; m < NV; ++m) {
     double t = ps.part[parity][0][m];
     for (int r = 1; r < C; ++r) t = t + ps.part[parity][r][m];
     v[m] = t;
   }
+  return ok;
 }
 
 // y = A x at compact cell c (own), the reference's expression order; the
@@ -150,15 +207,21 @@ __device__ __forceinline__ double dsm_row(const MeshDims& d, const Dsm& m, int o
   return y;
 }
 
-template <bool SYM>
+template <bool SYM, bool MB>
 __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
   const MeshDims& d = a.d;
   const SysF64& s = a.s;
   const int rank = m.rank;
+  Exchange xc;
+  xc.C = C;
+  xc.rank = rank;
+  xc.parity = 0;
+  xc.phase = 0;
+  xc.err = a.ws.err;
+  xc.timeout_ns = a.timeout_ns;
   const int begin = min(d.n, rank * a.chunk);
   const int end = min(d.n, begin + a.chunk);
   const int B = blockDim.x;
-  int parity = 0;
 
   // Load the slice; the symmetric form's west/south/bottom links are the
   // neighbours' east/north/top links (zero at the r and z walls, where the
@@ -197,13 +260,12 @@ __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
     v3[1] = v3[1] + rv * rv;
     v3[2] = v3[2] + rv * zv;
   }
-  dsm_allsum<3>(v3, ps, C, rank, parity);
-  parity ^= 1;
+  bool ok = dsm_allsum<3, MB>(v3, ps, xc);
   const double bnorm = sqrt(v3[0]);
   double residual = 0.0;
   int n_iter = 0;
   bool nan_fill = false;
-  if (!(bnorm < kSmall)) {
+  if (ok && !(bnorm < kSmall)) {
     double rz = v3[2];
     double beta = 0.0;
     residual = sqrt(v3[1]) / bnorm;
@@ -238,8 +300,7 @@ __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
           v1[0] = v1[0] + pc * qv;
         }
       }
-      dsm_allsum<1>(v1, ps, C, rank, parity);
-      parity ^= 1;
+      if (!(ok = dsm_allsum<1, MB>(v1, ps, xc))) break;
       const double pq = v1[0];
       if (fabs(pq) < kSmall) break;
       const double alpha = rz / pq;
@@ -262,8 +323,7 @@ __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
           v2[1] = v2[1] + rn * zv;
         }
       }
-      dsm_allsum<2>(v2, ps, C, rank, parity);
-      parity ^= 1;
+      if (!(ok = dsm_allsum<2, MB>(v2, ps, xc))) break;
       residual = sqrt(v2[0]) / bnorm;
       n_iter = iter;
       if (residual < a.tol) break;
@@ -282,7 +342,8 @@ __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
   }
   if (rank == 0 && threadIdx.x == 0) {
     SolveResult* res = a.ws.result;
-    res->status = isfinite(residual) ? EAF_OK : EAF_ENONFINITE;
+    const int err = ld_volatile_i32(a.ws.err);
+    res->status = err != 0 ? err : (isfinite(residual) ? EAF_OK : EAF_ENONFINITE);
     res->n_iter = n_iter;
     res->n_outer = 0;
     res->sym = SYM ? 1 : 0;
@@ -291,9 +352,10 @@ __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
   }
 }
 
+template <bool MB>
 __global__ void __launch_bounds__(1024, 1) cg_dsm_kernel(DsmArgs a) {
   extern __shared__ __align__(16) double dsm_smem[];
-  __shared__ PartSmem ps;
+  __shared__ __align__(8) PartSmem ps;
   Dsm m;
   m.base = dsm_smem;
   m.base_sa = smem_addr(dsm_smem);
@@ -301,12 +363,21 @@ __global__ void __launch_bounds__(1024, 1) cg_dsm_kernel(DsmArgs a) {
   m.rank = (int)cluster_ctarank();
   m.fd = a.fd_chunk;
   const int C = (int)cluster_nctarank();
-  // Every block has started before any block addresses another's memory.
+  if (MB && threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&ps.bar[0])), "r"(C)
+                 : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&ps.bar[1])), "r"(C)
+                 : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // Every block has started (and initialised its barriers) before any
+  // block addresses another's memory.
   cluster_sync_all();
   if (*a.s.asym == 0)
-    dsm_body<true>(a, m, ps, C);
+    dsm_body<true, MB>(a, m, ps, C);
   else
-    dsm_body<false>(a, m, ps, C);
+    dsm_body<false, MB>(a, m, ps, C);
+  // No block leaves while another may still address its shared memory.
   cluster_sync_all();
 }
 
@@ -328,7 +399,7 @@ int dsm_max_cells(int cluster) {
 
 cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs& ws,
                               int max_iter, double tol, int block, int cluster,
-                              cudaStream_t st) {
+                              cudaStream_t st, int signal, uint64_t timeout_ns) {
   if (cluster < 1 || cluster > kMaxClusterSize || block < 32 || block > 1024 ||
       block % 32 != 0 || d.n > dsm_max_cells(cluster))
     return cudaErrorInvalidValue;
@@ -338,12 +409,15 @@ cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs&
   a.ws = ws;
   a.max_iter = max_iter;
   a.tol = tol;
+  a.timeout_ns = timeout_ns;
   a.chunk = (d.n + cluster - 1) / cluster;
   a.fd_chunk = FastDiv((uint32_t)a.chunk);
   const size_t smem = dsm_smem_bytes(a.chunk);
-  const void* k = (const void*)cg_dsm_kernel;
+  const void* k = signal == kDsmSignalClusterBarrier ? (const void*)cg_dsm_kernel<false>
+                                                      : (const void*)cg_dsm_kernel<true>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
   if (e == cudaSuccess && cluster > 8)
     e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;

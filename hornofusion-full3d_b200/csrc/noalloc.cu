@@ -179,7 +179,7 @@ extern "C" int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device,
   eaf::HaloInputs in = {aW, aE, aS, aN, aB, aT, aP, Su, phi};
   e = eaf::launch_pack_f64(d, in, s, st);
   if (e == cudaSuccess)
-    e = eaf::launch_f64_solver(L, true, d, s, ws, (size_t)kPartSlots * kNoallocMaxBlocks,
+    e = eaf::launch_f64_solver(L, 1, d, s, ws, (size_t)kPartSlots * kNoallocMaxBlocks,
                                max_iter, tol, kNoallocTimeoutNs, st);
   if (e == cudaSuccess) e = eaf::launch_unpack_f64(d, s.x, phi, st);
   eaf::SolveResult r;

@@ -151,10 +151,12 @@ int eaf_cg_last_cluster(eaf_cg_t h, int* cluster_blocks);
 
 /* A launch that is ONE cluster (grid == cluster blocks) on a mesh that fits
  * the cluster's shared memory (about 35,000 cells at 16 blocks) runs, by
- * default (resident = 1), the cluster-resident kernel: the whole system
- * lives in distributed shared memory for the whole solve and an iteration
- * touches no global memory. It gives the same bits as the global-memory
- * cluster kernel on that launch (resident = 0). No reference counterpart. */
+ * default, the cluster-resident kernel: the whole system lives in
+ * distributed shared memory for the whole solve and an iteration touches no
+ * global memory. resident = 1: its blocks signal their partials by remote
+ * mbarrier arrivals (default); 2: by a full cluster barrier; 0: run the
+ * global-memory cluster kernel instead. All give the same bits on one
+ * launch. No reference counterpart. */
 int eaf_cg_set_resident(eaf_cg_t h, int resident);
 
 /* Kernel of the plain FP64 solve on a flat (cluster-free) grid: per-thread
@@ -411,6 +413,12 @@ int eaf_batch_set_width(eaf_batch_t b, int sys, int width);
 int eaf_batch_lane_width(eaf_batch_t b, int sys, int* width);
 /* Plans lanes and queues (done by the first solve otherwise). */
 int eaf_batch_plan(eaf_batch_t b, int* grid, int* block, int* nlanes);
+/* Launch whose association a system's FP64 dot products follow (the
+ * oracle's plan): its lane (width blocks of 512 threads) or, for a system of
+ * at least 300,000 cells without an explicit width, the single-system
+ * launch of its mesh: such systems run after the batched launch, one after
+ * another over the whole GPU, in the same graph. */
+int eaf_batch_system_plan(eaf_batch_t b, int sys, int* grid, int* block, int* cluster);
 /* Host inputs of one system, uploaded on the batch stream (phi is the
  * warm start and, after a solve, is read back with eaf_batch_get_phi). */
 int eaf_batch_set_system(eaf_batch_t b, int sys, const double* aW,

@@ -108,3 +108,31 @@ def test_batch_width_override_and_replay():
         b.set_system(0, s2.arrays(), g.zeros_phi(12, 24, 16))
         b.solve()
         assert b.result(0)[0] < 1e-8 and b.result(0) != first[0]
+
+
+def test_large_system_runs_at_full_width_after_the_lanes():
+    """A 60x120x84 system (over the large-system threshold) is solved after
+    the batched launch with its single-system launch: bit-identical to the
+    oracle with that plan, and to the same system alone; the small systems
+    of the batch keep their lanes."""
+    import oracle
+    g = gen()
+    big = g.make_system(60, 120, 84, 24, seed=11)
+    sl = [big] + systems()[:3]
+    eaf = pkg()
+    dims = [(s.nr, s.nth, s.nz) for s in sl]
+    with eaf.Batch(dims) as b:
+        plans = [b.system_plan(i) for i in range(len(sl))]
+    with eaf.CGSolver(60, 120, 84) as cg:
+        cg.solve(big.arrays(), g.zeros_phi(60, 120, 84), 1, 1e-8)
+        single = cg.last_launch()
+    assert plans[0] == single and plans[1][1] == 512
+    st, res, phis, lw = run_batch(sl)
+    assert st == 0
+    for i, s in enumerate(sl):
+        ref = g.zeros_phi(s.nr, s.nth, s.nz)
+        ro, no = oracle.cg(s, ref, 200000, 1e-8, plan=plans[i])
+        assert (res[i][1], res[i][0]) == (no, ro), i
+        assert np.array_equal(phis[i], ref)
+    st1, res1, phis1, _ = run_batch([big])
+    assert res1[0] == res[0] and np.array_equal(phis1[0], phis[0])

@@ -156,14 +156,17 @@ def test_resident_kernel_matches_global_cluster_kernel_and_oracle(dims, block, c
     g = gen()
     s = g.make_system(*dims, seed=4)
     phi_r = g.zeros_phi(*dims[:3])
-    (res_r, nit_r, st_r), plan = _solve_resident(s, phi_r, 100000, TOL, block, cluster, True)
+    (res_r, nit_r, st_r), plan = _solve_resident(s, phi_r, 100000, TOL, block, cluster, 1)
     phi_g = g.zeros_phi(*dims[:3])
-    (res_g, nit_g, st_g), plan_g = _solve_resident(s, phi_g, 100000, TOL, block, cluster,
-                                                   False)
+    (res_g, nit_g, st_g), plan_g = _solve_resident(s, phi_g, 100000, TOL, block, cluster, 0)
     assert plan == plan_g == (cluster, block, cluster)
     assert st_r == st_g == 0 and res_r < TOL
     assert (nit_r, res_r) == (nit_g, res_g)
     assert np.array_equal(phi_r, phi_g)
+    phi_b = g.zeros_phi(*dims[:3])           # cluster-barrier signalling
+    (res_b, nit_b, st_b), plan_b = _solve_resident(s, phi_b, 100000, TOL, block, cluster, 2)
+    assert plan_b == plan and (nit_b, res_b, st_b) == (nit_r, res_r, 0)
+    assert np.array_equal(phi_b, phi_r)
     phi_o = g.zeros_phi(*dims[:3])
     assert oracle.cg(s, phi_o, 100000, TOL, plan=plan) == (res_r, nit_r)
     assert np.array_equal(phi_r, phi_o)
