@@ -271,14 +271,14 @@ class CGSolver:
         check(self._lib.eaf_cg_set_cluster(self._h, int(cluster)), "set_cluster")
 
     RESIDENT_OFF = 0
-    RESIDENT_MBARRIER = 1
-    RESIDENT_CLUSTER_BARRIER = 2
+    RESIDENT_CLUSTER_BARRIER = 1
+    RESIDENT_MBARRIER = 2
 
     def set_resident(self, mode: int = 1) -> None:
         """One-cluster launches of a mesh that fits keep the system in the
-        cluster's shared memory, the blocks signalling their partials by
-        mbarrier arrivals (RESIDENT_MBARRIER, default) or a cluster barrier
-        (RESIDENT_CLUSTER_BARRIER), or run the global-memory cluster kernel
+        cluster's shared memory, the blocks signalling their partials by a
+        cluster barrier (RESIDENT_CLUSTER_BARRIER, default) or mbarrier
+        arrivals (RESIDENT_MBARRIER), or run the global-memory cluster kernel
         (RESIDENT_OFF); all give the same bits."""
         check(self._lib.eaf_cg_set_resident(self._h, int(mode)), "set_resident")
 

@@ -101,9 +101,10 @@ namespace eaf {
 
 // Launch shape for a persistent kernel over n cells: an explicit
 // eaf_cg_set_launch shape, else the tuned shape of this mesh (FP64 solver),
-// else one 1024-thread block up to 8192 cells or one 512-thread block per
-// 2048 cells; capped by co-residency of the kernel (variant) that runs
-// blocks of that size. The reference-form FP64 solver may run on a grid of
+// else, for the reference-form FP64 solver on a mesh that fits, one
+// cluster-resident launch (below), else one 1024-thread block up to 8192
+// cells or one 512-thread block per 2048 cells; capped by co-residency of
+// the kernel (variant) that runs blocks of that size. The reference-form FP64 solver may run on a grid of
 // thread-block clusters (eaf_cg_set_cluster, else the tuned cluster size):
 // the grid is then a whole number of clusters, at most as many as can be
 // resident; a cluster size the device cannot launch falls back to none.
@@ -118,7 +119,8 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
   int g;
   int tb = 0, tg = 0, tc = 1, ts = 0;
   const bool automatic = req_block == 0 && req_grid == 0;
-  if (automatic && f64 && tuned_single_launch(nr, nth, nz, &tb, &tg, &tc, &ts)) {
+  const bool tuned = automatic && f64 && tuned_single_launch(nr, nth, nz, &tb, &tg, &tc, &ts);
+  if (tuned) {
     b = tb;
     g = tg;
   } else if (req_grid > 0) {
@@ -131,6 +133,20 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
     g = (int)(want < 1 ? 1 : want);
   }
   int c = 1;
+  if (automatic && f64 && form == EAF_CG_FORM_REFERENCE && !tuned && req_cluster == 0) {
+    // A small mesh outside the table: one cluster that keeps the system in
+    // its shared memory (8 blocks up to 8192 cells, else 16), one cell per
+    // thread up to 640 cells a block, else two.
+    const int cs = n <= 8192 ? 8 : 16;
+    if (n <= dsm_max_cells(cs) && max_active_clusters(512, n, cs) >= 1) {
+      const long long per = (n + cs - 1) / cs;
+      long long t = per <= 640 ? per : (per + 1) / 2;
+      t = ((t + 31) / 32) * 32;
+      b = (int)(t < 64 ? 64 : (t > 1024 ? 1024 : t));
+      g = cs;
+      tc = cs;
+    }
+  }
   if (f64 && form == EAF_CG_FORM_REFERENCE) {
     c = req_cluster > 0 ? req_cluster : (automatic ? tc : 1);
     if (c > 1) {
@@ -177,7 +193,7 @@ cudaError_t launch_f64_solver(const SolverLaunch& L, int resident, const MeshDim
                               int max_iter, double tol, uint64_t timeout_ns, cudaStream_t st) {
   if (runs_resident(L, d.n, resident != 0))
     return launch_cg_f64_dsm(d, s, ws, max_iter, tol, L.block, L.cluster, st,
-                             resident == 2 ? kDsmSignalClusterBarrier : kDsmSignalMbarrier,
+                             resident == 2 ? kDsmSignalMbarrier : kDsmSignalClusterBarrier,
                              timeout_ns);
   if (L.cluster > 1)
     return launch_cg_f64_cluster(d, s, ws, ws.part, slot_doubles, max_iter, tol, timeout_ns,

@@ -19,10 +19,11 @@
 //     folds the C partials in rank order. The association is that of the
 //     cluster all-reduce with one cluster (the oracle's plan (C, B, C)), so
 //     the solve is bit-identical to cg_cluster_kernel on the same launch
-//     shape and to the oracle. The signal is either a remote arrival on an
-//     mbarrier of each block (release at cluster scope, one arrival per
-//     block and phase, barriers double-buffered by all-reduce parity; the
-//     default) or a full cluster barrier.
+//     shape and to the oracle. The signal is either a full cluster barrier
+//     (the default: measured faster, 3.6 against 4.1 us per iteration at
+//     12x24x16) or a remote arrival on an mbarrier of each block (release at
+//     cluster scope, one arrival per block and phase, barriers
+//     double-buffered by all-reduce parity).
 //
 // Global memory is read once (the packed system) and written once (x and
 // the result). There is no global synchronisation and no wait that another
@@ -413,8 +414,8 @@ cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs&
   a.chunk = (d.n + cluster - 1) / cluster;
   a.fd_chunk = FastDiv((uint32_t)a.chunk);
   const size_t smem = dsm_smem_bytes(a.chunk);
-  const void* k = signal == kDsmSignalClusterBarrier ? (const void*)cg_dsm_kernel<false>
-                                                      : (const void*)cg_dsm_kernel<true>;
+  const void* k = signal == kDsmSignalMbarrier ? (const void*)cg_dsm_kernel<true>
+                                                : (const void*)cg_dsm_kernel<false>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);

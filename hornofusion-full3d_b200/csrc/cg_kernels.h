@@ -110,13 +110,14 @@ int max_active_clusters(int block, long long n, int cluster);
 // the whole system for the whole solve (cg_dsm.cu); bit-identical to the
 // cluster kernel on the launch (cluster, block, cluster). Meshes of at most
 // dsm_max_cells(cluster) cells (about 35,000 at 16 blocks on B200).
-// `signal` picks how a block signals its partials: kDsmSignalMbarrier
-// (remote mbarrier arrivals, default) or kDsmSignalClusterBarrier.
-constexpr int kDsmSignalMbarrier = 1;
-constexpr int kDsmSignalClusterBarrier = 2;
+// `signal` picks how a block signals its partials: kDsmSignalClusterBarrier
+// (a full cluster barrier, default: measured faster) or kDsmSignalMbarrier
+// (remote mbarrier arrivals).
+constexpr int kDsmSignalClusterBarrier = 1;
+constexpr int kDsmSignalMbarrier = 2;
 cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs& ws,
                               int max_iter, double tol, int block, int cluster,
-                              cudaStream_t st, int signal = kDsmSignalMbarrier,
+                              cudaStream_t st, int signal = kDsmSignalClusterBarrier,
                               uint64_t timeout_ns = 2000000000ull);
 int dsm_max_cells(int cluster);
 
@@ -135,8 +136,8 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
 bool runs_resident(const SolverLaunch& L, long long n, bool allowed);
 // Enqueues the plain FP64 solver (reference form) on launch L: the flat,
 // cluster or cluster-resident kernel; `slot_doubles` is the size of ws.part.
-// `resident`: 0 never the cluster-resident kernel, 1 it with mbarrier
-// signalling, 2 it with cluster-barrier signalling.
+// `resident`: 0 never the cluster-resident kernel, 1 it with cluster-barrier
+// signalling, 2 it with mbarrier signalling.
 cudaError_t launch_f64_solver(const SolverLaunch& L, int resident, const MeshDims& d,
                               const SysF64& s, const GroupWs& ws, size_t slot_doubles,
                               int max_iter, double tol, uint64_t timeout_ns, cudaStream_t st);

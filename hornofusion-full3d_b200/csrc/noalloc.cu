@@ -45,8 +45,9 @@ constexpr int kNoallocMaxCells = EAF_NOALLOC_MAX_CELLS;
 // Blocks of the largest launch this entry makes; the partial table is sized
 // for it. Every launch shape the handle entries pick for a mesh of at most
 // kNoallocMaxCells cells must fit, or the two would not give the same bits:
-// the tuned shapes (checked here) and the fallback of one 512-thread block
-// per 2048 cells.
+// the tuned shapes (checked here), the small-mesh fallback of one cluster
+// of at most 16 blocks, and the fallback without clusters of one 512-thread
+// block per 2048 cells (checked here).
 constexpr int kNoallocMaxBlocks = 64;
 static_assert(eaf::max_tuned_grid_up_to(kNoallocMaxCells) <= kNoallocMaxBlocks,
               "a tuned launch for a mesh within the no-allocation limit has more "

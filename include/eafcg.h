@@ -153,8 +153,8 @@ int eaf_cg_last_cluster(eaf_cg_t h, int* cluster_blocks);
  * the cluster's shared memory (about 35,000 cells at 16 blocks) runs, by
  * default, the cluster-resident kernel: the whole system lives in
  * distributed shared memory for the whole solve and an iteration touches no
- * global memory. resident = 1: its blocks signal their partials by remote
- * mbarrier arrivals (default); 2: by a full cluster barrier; 0: run the
+ * global memory. resident = 1: its blocks signal their partials by a full
+ * cluster barrier (default); 2: by remote mbarrier arrivals; 0: run the
  * global-memory cluster kernel instead. All give the same bits on one
  * launch. No reference counterpart. */
 int eaf_cg_set_resident(eaf_cg_t h, int resident);

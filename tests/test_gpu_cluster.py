@@ -163,7 +163,7 @@ def test_resident_kernel_matches_global_cluster_kernel_and_oracle(dims, block, c
     assert st_r == st_g == 0 and res_r < TOL
     assert (nit_r, res_r) == (nit_g, res_g)
     assert np.array_equal(phi_r, phi_g)
-    phi_b = g.zeros_phi(*dims[:3])           # cluster-barrier signalling
+    phi_b = g.zeros_phi(*dims[:3])           # mbarrier signalling
     (res_b, nit_b, st_b), plan_b = _solve_resident(s, phi_b, 100000, TOL, block, cluster, 2)
     assert plan_b == plan and (nit_b, res_b, st_b) == (nit_r, res_r, 0)
     assert np.array_equal(phi_b, phi_r)
