@@ -29,8 +29,9 @@ Further lines (--workload; one JSON line each, not the headline):
   pstep     one whole pressure step: assembly, CG, corrections
   fixed     a fixed amount of work for profiling and per-iteration timing:
             --repeat solves of exactly --iters CG iterations on --mesh
-            (tol 0), or --batch-size systems of the batch mix, or
-            --tdma-sweeps sweeps with --fixed-tdma
+            (tol 0; --launch, --cluster and --kernel pick the form), or
+            --batch-size systems of the batch mix, or --tdma-sweeps sweeps
+            with --fixed-tdma
 --cg-form selects the FP64 CG's recurrences (reference: two all-reduces per
 iteration, the default; one-reduction: the Chronopoulos-Gear form).
 """
@@ -1001,6 +1002,8 @@ def run_fixed(args):
                 cg.set_launch(*args.launch)
             if args.cluster is not None:
                 cg.set_cluster(args.cluster)
+            if args.kernel is not None:
+                cg.set_kernel({"loads": cg.KERNEL_LOADS, "stream": cg.KERNEL_STREAM}[args.kernel])
             for _ in range(args.repeat):
                 phi.zero_()
                 torch.cuda.synchronize()
@@ -1071,6 +1074,8 @@ def main(argv=None):
     ap.add_argument("--launch", type=int, nargs=2, default=None, metavar=("BLOCK", "GRID"))
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--batch-size", type=int, default=0)
+    ap.add_argument("--kernel", choices=["loads", "stream"], default=None,
+                    help="FP64 kernel on a flat grid (default: the tuned choice)")
     ap.add_argument("--fixed-tdma", action="store_true")
     args = ap.parse_args(argv)
     if args.workload == "batch" and args.impl == "ours" and _env_int("WORLD_SIZE", 1) > 1:
