@@ -895,10 +895,18 @@ def run_batch(args):
 
 def run_serve(args):
     """Poisson arrivals of simulated furnace runs (serving mix), 50 warm-
-    started solves per run, continuous batching; p50/p99 per rate."""
+    started solves per run, continuous batching; p50/p99 per rate.
+
+    Under torchrun (N ranks, one GPU each) every rank serves its own stream
+    of rate lambda/N on its own GPU (runs never span GPUs); the line reports
+    all solves over the slowest rank's wall time and p50/p99 over every
+    rank's client-observed latencies."""
     eaf = importlib.import_module(PKG)
     g = importlib.import_module(PKG + ".eafgen")
     sc = importlib.import_module(PKG + ".serve_client")
+    mg = importlib.import_module(PKG + ".multigpu")
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
     mix = g.SERVE_MIX
     pool = sc.build_pool(g, eaf, mix, 4, 0)
     rates = [float(r) for r in args.rates.split(",")]
@@ -908,13 +916,21 @@ def run_serve(args):
                         max_iter=args.mixed_inner if mixed else MAX_ITER, tol=TOL,
                         max_outer=args.mixed_outer, inner_tol=0.1) as srv:
             for rate in (rates if not mixed else rates[:1]):
-                st = sc.run_stream(srv, g, eaf, pool, mix, rate,
-                                   duration=args.serve_runs / rate, solves=args.solves_per_run,
-                                   seed=int(rate * 100), max_wall=900.0)
-                st.update({"rate_runs_per_s": rate, "mixed": mixed})
+                def stream():
+                    return sc.run_stream(srv, g, eaf, pool, mix, rate / world,
+                                         duration=args.serve_runs / rate,
+                                         solves=args.solves_per_run,
+                                         seed=int(rate * 100) + 7919 * rank, max_wall=900.0)
+                per_rank = mg.gather_outcomes(stream)
+                st = {k: v for k, v in per_rank[0].items() if k != "client_latency_ms"}
+                if world > 1:
+                    st = sc.merge_streams(per_rank)
+                    st["p50_ms"], st["p99_ms"] = st["client_p50_ms"], st["client_p99_ms"]
+                    st["mean_ms"] = float(np.mean(np.concatenate(
+                        [r["client_latency_ms"] for r in per_rank])))
+                st.update({"rate_runs_per_s": rate, "mixed": mixed, "gpus": world})
                 points.append(st)
     # plain FP64 per-solve path on the same pool, one solve at a time
-    import numpy as np
     per = {}
     for (dims, share) in mix:
         nr, nth, nz, _ = dims
@@ -926,6 +942,8 @@ def run_serve(args):
                 cg.solve(arrs, phi, MAX_ITER, TOL)
                 times.append(cg.last_timing()["e2e_ms"])
             per[str([nr, nth, nz])] = float(np.mean(times[1:] if len(times) > 1 else times))
+    if rank != 0:
+        return 0
     mean_ms = sum(share * per[str(list(d[:3]))] for d, share in mix)
     first = [p for p in points if not p["mixed"]]
     best = max(first, key=lambda p: p["solves_per_s"])
@@ -935,7 +953,9 @@ def run_serve(args):
                       {"mix": [[list(d[:3]), sh] for d, sh in mix],
                        "solves_per_run": args.solves_per_run,
                        "runs_per_rate": args.serve_runs,
-                       "rates_runs_per_s": rates, "budget_gb": 150})
+                       "rates_runs_per_s": rates, "budget_gb": 150,
+                       "parallelism": f"one stream of rate/{world} per GPU"})
+    line["n_gpus"] = world
     line["higher_is_better"] = False
     line["points"] = points
     line["per_solve_fp64"] = {"mean_ms_by_mesh": per, "mix_mean_ms": mean_ms,
@@ -1078,8 +1098,9 @@ def main(argv=None):
                     help="FP64 kernel on a flat grid (default: the tuned choice)")
     ap.add_argument("--fixed-tdma", action="store_true")
     args = ap.parse_args(argv)
-    if args.workload == "batch" and args.impl == "ours" and _env_int("WORLD_SIZE", 1) > 1:
-        return run_sharded_workload(run_batch, args)
+    if (args.workload in ("batch", "serve") and args.impl == "ours"
+            and _env_int("WORLD_SIZE", 1) > 1):
+        return run_sharded_workload(run_batch if args.workload == "batch" else run_serve, args)
     if args.workload != "production" and args.impl == "ours":
         return {"fine": run_fine, "batch": run_batch, "serve": run_serve,
                 "tdma": run_tdma, "pcorr": run_pcorr,

@@ -103,40 +103,48 @@ class ShardError(RuntimeError):
     """A rank's share failed; raised on every rank of the collective."""
 
 
+def gather_outcomes(fn, group=None) -> list:
+    """Collective over `group` (or a single process when torch.distributed is
+    not initialised): run `fn()` on every rank and return every rank's result,
+    in rank order, on every rank. Each rank takes exactly one collective step
+    (an object all-gather of its error and result), also when `fn` raised, so
+    a failure on one rank cannot leave the others waiting: every rank then
+    raises ShardError naming the failed ranks."""
+    import torch.distributed as dist
+    on = dist.is_available() and dist.is_initialized()
+    err, out = None, None
+    try:
+        out = fn()
+    except Exception as exc:  # reported to every rank below
+        err = f"{type(exc).__name__}: {exc}"
+    if on:
+        gathered = [None] * dist.get_world_size(group)
+        dist.all_gather_object(gathered, (err, out), group=group)
+    else:
+        gathered = [(err, out)]
+    failed = [(r, e) for r, (e, _) in enumerate(gathered) if e is not None]
+    if failed:
+        raise ShardError("; ".join(f"rank {r}: {e}" for r, e in failed))
+    return [o for _, o in gathered]
+
+
 def solve_sharded(items: list[Item], solve_share, group=None,
                   budget: float | None = None) -> tuple[float, dict, list[list[Item]]]:
-    """Collective over `group` (or a single process when torch.distributed is
-    not initialised): partition `items` across the ranks (`partition`), call
-    `solve_share(my_items) -> (elapsed_s, {key: result})` on every rank with
-    its share, and return (the slowest rank's elapsed seconds, the results
-    of every rank merged by key, the partition) on every rank.
-
-    Every rank takes exactly one collective step (an object all-gather of
-    its error, time and results), also when its solve raised, so a failure
-    on one rank cannot leave the others waiting: every rank then raises
-    ShardError naming the failed ranks."""
+    """Collective over `group`: partition `items` across the ranks
+    (`partition`), call `solve_share(my_items) -> (elapsed_s, {key: result})`
+    on every rank with its share, and return (the slowest rank's elapsed
+    seconds, the results of every rank merged by key, the partition) on every
+    rank; failures as in `gather_outcomes`."""
     import torch.distributed as dist
     on = dist.is_available() and dist.is_initialized()
     world = dist.get_world_size(group) if on else 1
     rank = dist.get_rank(group) if on else 0
     parts = partition(items, world, budget)
-    err, elapsed, local = None, 0.0, {}
-    try:
-        elapsed, local = solve_share(parts[rank])
-    except Exception as exc:  # reported to every rank below
-        err = f"{type(exc).__name__}: {exc}"
-    if on:
-        gathered = [None] * world
-        dist.all_gather_object(gathered, (err, float(elapsed), local), group=group)
-    else:
-        gathered = [(err, float(elapsed), local)]
-    failed = [(r, e) for r, (e, _, _) in enumerate(gathered) if e is not None]
-    if failed:
-        raise ShardError("; ".join(f"rank {r}: {e}" for r, e in failed))
+    outs = gather_outcomes(lambda: solve_share(parts[rank]), group)
     merged: dict = {}
-    for _, _, p in gathered:
+    for _, p in outs:
         overlap = set(merged) & set(p)
         if overlap:
             raise RuntimeError(f"keys solved on two ranks: {sorted(overlap)[:5]}")
         merged.update(p)
-    return max(t for _, t, _ in gathered), merged, parts
+    return max(float(t) for t, _ in outs), merged, parts

@@ -75,6 +75,7 @@ def run_stream(srv, g, eaf, pool, mix, rate: float, duration: float, solves: int
     active = {}               # run id -> state
     done_runs = 0
     residuals = []
+    latencies = []            # client-observed submit-to-completion, ms
     while waiting or active:
         now = time.perf_counter() - t0
         if now > max_wall:
@@ -92,6 +93,7 @@ def run_stream(srv, g, eaf, pool, mix, rate: float, duration: float, solves: int
             phi[...] = 0.0
             st = {"dims": dims, "seed": rseed, "k": 0, "phi": phi}
             st["ticket"] = srv.submit(rid, pool[dims][rseed % len(pool[dims])], phi)
+            st["t_sub"] = time.perf_counter()
             active[rid] = st
         waiting = still
         for rid in list(active):
@@ -100,6 +102,7 @@ def run_stream(srv, g, eaf, pool, mix, rate: float, duration: float, solves: int
             if r is None:
                 continue
             residuals.append(r[0])
+            latencies.append(1e3 * (time.perf_counter() - st["t_sub"]))
             if r[3] != 0:
                 raise RuntimeError(f"run {rid} solve {st['k']} failed with status {r[3]}")
             st["k"] += 1
@@ -107,6 +110,7 @@ def run_stream(srv, g, eaf, pool, mix, rate: float, duration: float, solves: int
                 systems = pool[st["dims"]]
                 st["ticket"] = srv.submit(
                     rid, systems[(st["seed"] + st["k"]) % len(systems)], st["phi"])
+                st["t_sub"] = time.perf_counter()
             else:
                 srv.close_run(rid)
                 del active[rid]
@@ -115,8 +119,25 @@ def run_stream(srv, g, eaf, pool, mix, rate: float, duration: float, solves: int
     wall = time.perf_counter() - t0
     stats = srv.stats()
     stats.update({"runs": done_runs, "wall_s": wall,
-                  "max_residual": float(max(residuals)) if residuals else None})
+                  "max_residual": float(max(residuals)) if residuals else None,
+                  "client_latency_ms": latencies})
     return stats
+
+
+def merge_streams(per_rank: list) -> dict:
+    """Whole-job figures of streams served side by side on several GPUs (one
+    run_stream result per rank): solves over the slowest rank's wall time,
+    and p50/p99 over every rank's client-observed latencies."""
+    lat = np.sort(np.concatenate([np.asarray(r["client_latency_ms"], dtype=float)
+                                  for r in per_rank if r["client_latency_ms"]]))
+    pct = (lambda p: float(lat[min(len(lat) - 1, int(np.floor(p * (len(lat) - 1) + 0.5)))])
+           if len(lat) else None)
+    wall = max(r["wall_s"] for r in per_rank)
+    solves = sum(r["solves"] for r in per_rank)
+    return {"solves": solves, "wall_s": wall, "solves_per_s": solves / wall if wall else 0.0,
+            "client_p50_ms": pct(0.50), "client_p99_ms": pct(0.99),
+            "server_p99_ms_by_rank": [r.get("p99_ms") for r in per_rank],
+            "runs": sum(r["runs"] for r in per_rank)}
 
 
 def main(argv=None) -> int:

@@ -194,3 +194,50 @@ def test_solve_sharded_failure_on_one_rank_raises_everywhere(tmp_path):
     for r in range(2):
         out = json.load(open(tmp_path / f"out{r}.json"))
         assert out == {"error": "rank 1: RuntimeError: device lost"}
+
+
+def test_merge_streams_whole_job_figures():
+    """Streams served side by side on two GPUs: solves over the slowest
+    rank's wall time, percentiles over every rank's latencies."""
+    import importlib
+    sc = importlib.import_module("hornofusion-full3d_b200.serve_client")
+    a = {"solves": 3, "wall_s": 2.0, "runs": 1, "p99_ms": 9.0,
+         "client_latency_ms": [1.0, 2.0, 3.0]}
+    b = {"solves": 2, "wall_s": 4.0, "runs": 1, "p99_ms": 30.0,
+         "client_latency_ms": [10.0, 30.0]}
+    m = sc.merge_streams([a, b])
+    assert m["solves"] == 5 and m["wall_s"] == 4.0 and m["solves_per_s"] == 1.25
+    assert m["client_p50_ms"] == 3.0 and m["client_p99_ms"] == 30.0
+    assert m["server_p99_ms_by_rank"] == [9.0, 30.0] and m["runs"] == 2
+
+
+def _outcome_worker(rank, world, port, out_dir):
+    import sys
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import datetime
+    import json
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        m = mg()
+        outs = m.gather_outcomes(lambda: {"rank": rank, "square": rank * rank})
+        with open(os.path.join(out_dir, f"g{rank}.json"), "w") as f:
+            json.dump(outs, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_outcomes_three_ranks(tmp_path):
+    import json
+
+    import torch.multiprocessing as mp
+    mp.start_processes(_outcome_worker, args=(3, _free_port(), str(tmp_path)), nprocs=3,
+                       join=True, start_method="spawn")
+    want = [{"rank": r, "square": r * r} for r in range(3)]
+    for r in range(3):
+        assert json.load(open(tmp_path / f"g{r}.json")) == want
