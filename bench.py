@@ -1023,7 +1023,8 @@ def run_fixed(args):
             if args.cluster is not None:
                 cg.set_cluster(args.cluster)
             if args.kernel is not None:
-                cg.set_kernel({"loads": cg.KERNEL_LOADS, "stream": cg.KERNEL_STREAM}[args.kernel])
+                cg.set_kernel({"loads": cg.KERNEL_LOADS, "stream": cg.KERNEL_STREAM,
+                               "slots": cg.KERNEL_SLOTS}[args.kernel])
             for _ in range(args.repeat):
                 phi.zero_()
                 torch.cuda.synchronize()
@@ -1094,7 +1095,7 @@ def main(argv=None):
     ap.add_argument("--launch", type=int, nargs=2, default=None, metavar=("BLOCK", "GRID"))
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--batch-size", type=int, default=0)
-    ap.add_argument("--kernel", choices=["loads", "stream"], default=None,
+    ap.add_argument("--kernel", choices=["loads", "stream", "slots"], default=None,
                     help="FP64 kernel on a flat grid (default: the tuned choice)")
     ap.add_argument("--fixed-tdma", action="store_true")
     args = ap.parse_args(argv)

@@ -163,8 +163,10 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
       }
     }
   }
-  int stream = 0;
-  if (f64 && form == EAF_CG_FORM_REFERENCE && c == 1) {
+  int stream = 0, slots = 0;
+  if (f64 && form == EAF_CG_FORM_REFERENCE && c == 1 && req_kernel == EAF_CG_KERNEL_SLOTS)
+    slots = 1;
+  if (f64 && form == EAF_CG_FORM_REFERENCE && c == 1 && !slots) {
     stream = req_kernel == EAF_CG_KERNEL_STREAM ? 1
              : req_kernel == EAF_CG_KERNEL_LOADS ? 0
                                                  : (automatic ? ts : 0);
@@ -181,6 +183,8 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
   L.block = b;
   L.cluster = c;
   L.stream = stream;
+  L.slots = slots;
+  if (slots && g > kMaxClusters) L.grid = kMaxClusters;
   return L;
 }
 
@@ -195,7 +199,7 @@ cudaError_t launch_f64_solver(const SolverLaunch& L, int resident, const MeshDim
     return launch_cg_f64_dsm(d, s, ws, max_iter, tol, L.block, L.cluster, st,
                              resident == 2 ? kDsmSignalMbarrier : kDsmSignalClusterBarrier,
                              timeout_ns);
-  if (L.cluster > 1)
+  if (L.cluster > 1 || L.slots)
     return launch_cg_f64_cluster(d, s, ws, ws.part, slot_doubles, max_iter, tol, timeout_ns,
                                  L.grid, L.block, L.cluster, st);
   if (L.stream)
@@ -366,14 +370,15 @@ int eaf_cg_mixed_trace(eaf_cg_t h, double* steps, int max_steps, int* n_steps) {
 }
 
 int eaf_cg_set_kernel(eaf_cg_t h, int kernel) {
-  if (!h || kernel < EAF_CG_KERNEL_AUTO || kernel > EAF_CG_KERNEL_STREAM) return EAF_EINVAL;
+  if (!h || kernel < EAF_CG_KERNEL_AUTO || kernel > EAF_CG_KERNEL_SLOTS) return EAF_EINVAL;
   h->kernel = kernel;
   return EAF_OK;
 }
 
 int eaf_cg_last_kernel(eaf_cg_t h, int* kernel) {
   if (!h || !kernel) return EAF_EINVAL;
-  *kernel = h->last_stream ? EAF_CG_KERNEL_STREAM : EAF_CG_KERNEL_LOADS;
+  *kernel = h->last_stream == 2 ? EAF_CG_KERNEL_SLOTS
+            : h->last_stream ? EAF_CG_KERNEL_STREAM : EAF_CG_KERNEL_LOADS;
   return EAF_OK;
 }
 
@@ -498,7 +503,7 @@ int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts&
                                   h->st, h->trace_d));
   } else {
     const eaf::SolverLaunch L = pick_launch(h, true, &grid, &block, &cluster);
-    h->last_stream = L.stream;
+    h->last_stream = L.slots ? 2 : L.stream;
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     if (h->form == EAF_CG_FORM_ONE_REDUCTION)
       EAF_CUDA(eaf::launch_cg1_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,

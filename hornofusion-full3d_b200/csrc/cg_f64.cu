@@ -1126,7 +1126,7 @@ cudaError_t launch_cg_f64_cluster(const MeshDims& d, const SysF64& s, const Grou
                                   double* slots, size_t slot_doubles, int max_iter,
                                   double tol, uint64_t timeout_ns, int grid, int block,
                                   int cluster, cudaStream_t st) {
-  if (cluster < 2 || cluster > kMaxClusterSize || grid % cluster != 0 ||
+  if (cluster < 1 || cluster > kMaxClusterSize || grid % cluster != 0 ||
       grid / cluster > kMaxClusters || cluster_slot_doubles(grid / cluster) > slot_doubles)
     return cudaErrorInvalidValue;
   CgArgs a;

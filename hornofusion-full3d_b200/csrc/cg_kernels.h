@@ -126,6 +126,7 @@ int dsm_max_cells(int cluster);
 struct SolverLaunch {
   int grid, block, cluster;
   int stream = 0;  // 1: the bulk-copy streaming kernel (flat grids only)
+  int slots = 0;   // 1: flat grid, slot-polling all-reduce (clusters of one)
 };
 // The launch a handle with the requested shape (0 = automatic) uses on an
 // nr x nth x nz mesh (api.cu): the tuned shape, else the fallback rules,

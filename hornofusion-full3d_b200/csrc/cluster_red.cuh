@@ -18,9 +18,10 @@
 // Association (restated by the oracle's cluster plan): block partials as in
 // group_allsum; cluster partial cp = (((p_0 + p_1) + p_2) + ...) over the
 // cluster's blocks in rank order; one cluster: total = cp; otherwise lane l
-// of the leader warp sums cp_l, cp_{l+32} sequentially from 0.0 and the 32
-// lane sums are folded by the xor butterfly. With C = 1 this is exactly the
-// association of group_allsum.
+// of the leader warp sums cp_l, cp_{l+32}, ... sequentially from 0.0 and the
+// 32 lane sums are folded by the xor butterfly. With C = 1 this is exactly
+// the association of group_allsum: a flat grid whose all-reduce polls the
+// partials themselves instead of an arrival counter (EAF_CG_KERNEL_SLOTS).
 //
 // Memory ordering. Block writes are ordered before the block's cluster
 // barrier arrival (release, cluster scope); the leader acquires them at the
@@ -52,7 +53,8 @@
 namespace eaf {
 
 constexpr int kMaxClusterSize = 16;
-constexpr int kMaxClusters = 64;       // leaders: two slots per lane at most
+constexpr int kPerLane = 5;            // leaders' slots a lane reads
+constexpr int kMaxClusters = 32 * kPerLane;
 constexpr int kClusterSlotsNV = 4;     // sums per all-reduce, at most
 constexpr int kClusterSets = 3;
 // Signalling NaN (quiet bit clear, payload nonzero): the empty-slot marker.
@@ -210,19 +212,21 @@ __device__ __forceinline__ bool cluster_allsum(T (&v)[NV], ClusterGroup& g) {
 #pragma unroll
         for (int m = 0; m < NV; ++m) st_relaxed_f64(cur + m * stride + g.cl, cp[m]);
       }
-      // lane l reads the partials of clusters l and l + 32
-      double got[2][NV];
-      const bool has0 = lane < g.ncl, has1 = lane + 32 < g.ncl;
+      // lane l reads the partials of clusters l, l + 32, ...
+      double got[kPerLane][NV];
       uint64_t t0 = 0;
       uint32_t spins = 0;
       bool done = false;
       while (true) {
         bool mine = true;
 #pragma unroll
-        for (int m = 0; m < NV; ++m) {
-          got[0][m] = has0 ? ld_relaxed_f64(cur + m * stride + lane) : 0.0;
-          got[1][m] = has1 ? ld_relaxed_f64(cur + m * stride + lane + 32) : 0.0;
-          mine = mine && !is_marker(got[0][m]) && !is_marker(got[1][m]);
+        for (int u = 0; u < kPerLane; ++u) {
+          const int c = lane + 32 * u;
+#pragma unroll
+          for (int m = 0; m < NV; ++m) {
+            got[u][m] = c < g.ncl ? ld_relaxed_f64(cur + m * stride + c) : 0.0;
+            mine = mine && !is_marker(got[u][m]);
+          }
         }
         done = __all_sync(0xffffffffu, mine);
         if (done) break;
@@ -245,8 +249,9 @@ __device__ __forceinline__ bool cluster_allsum(T (&v)[NV], ClusterGroup& g) {
 #pragma unroll
       for (int m = 0; m < NV; ++m) {
         double s = 0.0;
-        if (has0) s = s + got[0][m];
-        if (has1) s = s + got[1][m];
+#pragma unroll
+        for (int u = 0; u < kPerLane; ++u)
+          if (lane + 32 * u < g.ncl) s = s + got[u][m];
         tot[m] = warp_allsum(s);
       }
     }

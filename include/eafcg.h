@@ -162,12 +162,17 @@ int eaf_cg_set_resident(eaf_cg_t h, int resident);
 /* Kernel of the plain FP64 solve on a flat (cluster-free) grid: per-thread
  * loads (EAF_CG_KERNEL_LOADS), or each phase's operands staged in shared
  * memory by bulk copies a few tiles ahead of use (EAF_CG_KERNEL_STREAM),
+ * or per-thread loads with a slot-polling all-reduce (EAF_CG_KERNEL_SLOTS),
  * or the tuned choice of the mesh (EAF_CG_KERNEL_AUTO). Both give the same
  * bits on the same launch shape. eaf_cg_last_kernel reports which ran. No
  * reference counterpart. */
 #define EAF_CG_KERNEL_AUTO 0
 #define EAF_CG_KERNEL_LOADS 1
 #define EAF_CG_KERNEL_STREAM 2
+/* per-thread loads, all-reduce by polling every block's partial in its slot
+ * (the cluster all-reduce with clusters of one block) instead of an arrival
+ * counter; same association, so the same bits as EAF_CG_KERNEL_LOADS */
+#define EAF_CG_KERNEL_SLOTS 3
 int eaf_cg_set_kernel(eaf_cg_t h, int kernel);
 int eaf_cg_last_kernel(eaf_cg_t h, int* kernel);
 

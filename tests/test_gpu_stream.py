@@ -107,6 +107,30 @@ def test_kernel_setting_is_validated():
     eaf = pkg()
     with eaf.CGSolver(12, 24, 16) as cg:
         with pytest.raises(eaf.EafError):
-            cg.set_kernel(3)
+            cg.set_kernel(4)
         with pytest.raises(eaf.EafError):
             cg.set_kernel(-1)
+
+
+@pytest.mark.parametrize("dims,block,grid,iters,tol", [((60, 120, 84, 24), 512, 148, 150, 0.0),
+                                                       ((35, 70, 50, 16), 256, 148, 100000, TOL),
+                                                       ((12, 24, 16, 8), 256, 8, 100000, TOL)])
+def test_slot_polling_all_reduce_bitwise(dims, block, grid, iters, tol):
+    """The flat grid whose all-reduce polls every block's partial in its slot
+    (clusters of one block): the same association as the counter form, so the
+    same bits as the per-thread-load kernel and the oracle's plan (G, B)."""
+    import oracle
+    eaf = pkg()
+    g = gen()
+    s = g.make_system(*dims, seed=1)
+    phi_s = g.zeros_phi(*dims[:3])
+    res_s, nit_s, st_s, plan, kern = solve(s, phi_s, iters, tol, block, grid,
+                                           eaf.CGSolver.KERNEL_SLOTS)
+    assert kern == eaf.CGSolver.KERNEL_SLOTS and plan == (grid, block)
+    phi_l = g.zeros_phi(*dims[:3])
+    res_l, nit_l, st_l, _, _ = solve(s, phi_l, iters, tol, block, grid,
+                                     eaf.CGSolver.KERNEL_LOADS)
+    assert (res_s, nit_s, st_s) == (res_l, nit_l, st_l) and np.array_equal(phi_s, phi_l)
+    phi_o = g.zeros_phi(*dims[:3])
+    assert oracle.cg(s, phi_o, iters, tol, plan=plan) == (res_s, nit_s)
+    assert np.array_equal(phi_s, phi_o)
