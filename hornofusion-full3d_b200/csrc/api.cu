@@ -138,11 +138,12 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
     // its shared memory (8 blocks up to 8192 cells, else 16), one cell per
     // thread up to 640 cells a block, else two.
     const int cs = n <= 8192 ? 8 : 16;
-    if (n <= dsm_max_cells(cs) && max_active_clusters(512, n, cs) >= 1) {
-      const long long per = (n + cs - 1) / cs;
-      long long t = per <= 640 ? per : (per + 1) / 2;
-      t = ((t + 31) / 32) * 32;
-      b = (int)(t < 64 ? 64 : (t > 1024 ? 1024 : t));
+    const long long per = (n + cs - 1) / cs;
+    long long t = per <= 640 ? per : (per + 1) / 2;
+    t = ((t + 31) / 32) * 32;
+    const int bs = (int)(t < 64 ? 64 : (t > 1024 ? 1024 : t));
+    if (dsm_can_launch(n, bs, cs) && max_active_clusters(bs, n, cs) >= 1) {
+      b = bs;
       g = cs;
       tc = cs;
     }
@@ -189,7 +190,8 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
 }
 
 bool runs_resident(const SolverLaunch& L, long long n, bool allowed) {
-  return allowed && L.cluster > 1 && L.grid == L.cluster && n <= dsm_max_cells(L.cluster);
+  return allowed && L.cluster > 1 && L.grid == L.cluster &&
+         dsm_can_launch(n, L.block, L.cluster);
 }
 
 cudaError_t launch_f64_solver(const SolverLaunch& L, int resident, const MeshDims& d,

@@ -398,6 +398,40 @@ int dsm_max_cells(int cluster) {
   return (int)(per_block * cluster);
 }
 
+bool dsm_can_launch(long long n, int block, int cluster) {
+  if (cluster < 1 || cluster > kMaxClusterSize || block < 32 || block > 1024 ||
+      block % 32 != 0 || n > dsm_max_cells(cluster))
+    return false;
+  const int chunk = (int)((n + cluster - 1) / cluster);
+  const size_t smem = dsm_smem_bytes(chunk);
+  const void* k = (const void*)cg_dsm_kernel<false>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess ||
+      (cluster > 8 &&
+       cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+           cudaSuccess)) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cluster);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int count = 0;
+  if (cudaOccupancyMaxActiveClusters(&count, k, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return count >= 1;
+}
+
 cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs& ws,
                               int max_iter, double tol, int block, int cluster,
                               cudaStream_t st, int signal, uint64_t timeout_ns) {

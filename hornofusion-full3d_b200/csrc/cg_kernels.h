@@ -120,6 +120,9 @@ cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs&
                               cudaStream_t st, int signal = kDsmSignalClusterBarrier,
                               uint64_t timeout_ns = 2000000000ull);
 int dsm_max_cells(int cluster);
+// Whether one cluster of `cluster` blocks of `block` threads holding an
+// n-cell system can be resident on the current device.
+bool dsm_can_launch(long long n, int block, int cluster);
 
 // Launch of a persistent single-system solver: blocks, threads per block,
 // blocks per thread-block cluster (1 = none).

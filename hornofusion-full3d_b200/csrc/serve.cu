@@ -19,7 +19,13 @@
 //     blocks than the device can keep resident, so no cooperative launch
 //     waits on blocks that another one occupies;
 //   * a run's lane width depends only on its mesh size, so each result is
-//     bit-identical whether the run is served alone or in any mix.
+//     bit-identical whether the run is served alone or in any mix;
+//   * large runs (at least kSoloCells cells, FP64) take no lane: when the
+//     oldest pending request is one, the server lets the device drain, then
+//     solves that request and the queued requests of its mesh one after
+//     another, each over the whole GPU with the single-system launch of its
+//     mesh (as the batch does with its large systems), while nothing else
+//     runs; their results are again the same alone and in any mix.
 //
 // Threading: any host thread may call the eaf_srv_* functions; one server
 // thread owns the launches and never holds the server lock while it enqueues
@@ -55,6 +61,7 @@ using Clock = std::chrono::steady_clock;
 namespace {
 
 constexpr int kSlots = 2;
+constexpr long long kSoloCells = 300000;
 
 struct SrvRun {
   int nr, nth, nz;
@@ -127,6 +134,7 @@ struct eaf_srv {
   double tol, inner_tol;
   uint64_t timeout_ns;
   int capacity, blocks_in_use;
+  int sms;
   std::mutex m;
   std::condition_variable cv, cv_done;
   std::thread th;
@@ -211,7 +219,11 @@ bool launch(eaf_srv* s, std::unique_lock<std::mutex>& lk) {
   // width class); requests of that mesh join in FIFO order while their
   // lanes fit. A batch's persistent launch ends when its slowest solve
   // does, so a batch of one mesh size keeps short solves from waiting on
-  // long ones; the second stream slot runs another size meanwhile.
+  // long ones; the second stream slot runs another size meanwhile. A large
+  // mesh waits for the whole device instead (see the file comment).
+  const SrvRun* oldest = s->runs[s->tickets[s->pending.front()].run];
+  const bool solo = !s->mixed && oldest->n >= kSoloCells;
+  if (solo && s->blocks_in_use != 0) return false;  // let the device drain
   std::vector<Pick> pick;
   std::vector<int> widths;
   std::vector<long long> cells;
@@ -230,7 +242,7 @@ bool launch(eaf_srv* s, std::unique_lock<std::mutex>& lk) {
       continue;
     }
     const int w = eaf::tuned_lane_width(r->nr, r->nth, r->nz);
-    if (used + w > free_blocks) break;
+    if (!solo && used + w > free_blocks) break;
     used += w;
     Pick p;
     p.id = *it;
@@ -245,12 +257,13 @@ bool launch(eaf_srv* s, std::unique_lock<std::mutex>& lk) {
   }
   if (pick.empty()) return false;
   // Blocks for this batch: no more than one lane per system needs, so the
-  // rest stay free for the next batch to run beside this one.
+  // rest stay free for the next batch to run beside this one; a batch of
+  // large runs holds the whole device.
   int want = 0;
   for (int w : widths) want += w;
-  const int G = std::min(free_blocks, want);
+  const int G = solo ? s->capacity : std::min(free_blocks, want);
   eaf::LanePlan lp;
-  if (eaf::plan_lanes(widths, cells, G, &lp) != EAF_OK) {
+  if (!solo && eaf::plan_lanes(widths, cells, G, &lp) != EAF_OK) {
     for (auto it = pick.rbegin(); it != pick.rend(); ++it) s->pending.push_front(it->id);
     return false;
   }
@@ -262,17 +275,20 @@ bool launch(eaf_srv* s, std::unique_lock<std::mutex>& lk) {
   for (const Pick& p : pick) sl->tickets.push_back(p.id);
   lk.unlock();
   const std::vector<int> tab = lp.packed();
-  memcpy(sl->h_tab, tab.data(), sizeof(int) * tab.size());
   const int nb = (int)pick.size();
-  for (int i = 0; i < nb; ++i) {
-    sl->h_sys[i] = pick[i].run->sys;
-    sl->h_sys[i].result = sl->d_res + i;
-  }
-  cudaError_t e = cudaMemcpyAsync(sl->d_tab, sl->h_tab, sizeof(int) * tab.size(),
-                                  cudaMemcpyHostToDevice, sl->st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(sl->d_sys, sl->h_sys, sizeof(BatchSys) * nb, cudaMemcpyHostToDevice,
+  cudaError_t e = cudaSuccess;
+  if (!solo) {
+    memcpy(sl->h_tab, tab.data(), sizeof(int) * tab.size());
+    for (int i = 0; i < nb; ++i) {
+      sl->h_sys[i] = pick[i].run->sys;
+      sl->h_sys[i].result = sl->d_res + i;
+    }
+    e = cudaMemcpyAsync(sl->d_tab, sl->h_tab, sizeof(int) * tab.size(), cudaMemcpyHostToDevice,
                         sl->st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sl->d_sys, sl->h_sys, sizeof(BatchSys) * nb, cudaMemcpyHostToDevice,
+                          sl->st);
+  }
   for (int i = 0; i < nb && e == cudaSuccess; ++i) {
     const SrvRun* r = pick[i].run;
     for (int k = 0; k < 8 && e == cudaSuccess; ++k)
@@ -283,11 +299,23 @@ bool launch(eaf_srv* s, std::unique_lock<std::mutex>& lk) {
     if (e == cudaSuccess) e = eaf::launch_pack_f64(r->sys.d, in, r->sys.s, sl->st);
   }
   const int nlanes = (int)lp.lane_first.size();
-  if (e == cudaSuccess)
+  if (solo) {
+    // one after another over the whole device, the single-system launch
+    for (int i = 0; i < nb && e == cudaSuccess; ++i) {
+      const SrvRun* r = pick[i].run;
+      eaf::SolverLaunch L = eaf::choose_launch(r->nr, r->nth, r->nz, s->sms, 0, 0, 0,
+                                               EAF_CG_FORM_REFERENCE, true);
+      L.stream = 0;  // a run's compact arrays carry no padding cell
+      const eaf::GroupWs ws = {sl->d_parts, sl->d_counters, sl->d_err, sl->d_res + i};
+      e = eaf::launch_f64_solver(L, 1, r->sys.d, r->sys.s, ws, (size_t)8 * s->capacity,
+                                 s->max_iter, s->tol, s->timeout_ns, sl->st);
+    }
+  }
+  if (e == cudaSuccess && !solo)
     e = cudaMemsetAsync(sl->d_counters, 0,
                         sizeof(unsigned long long) * eaf::kCounterStride * nlanes, sl->st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(sl->d_err, 0, sizeof(int), sl->st);
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && !solo) e = cudaMemsetAsync(sl->d_err, 0, sizeof(int), sl->st);
+  if (e == cudaSuccess && !solo) {
     const eaf::BatchTables tt = eaf::tables_from(sl->d_tab, G, nlanes, sl->d_sys,
                                                  sl->d_counters, sl->d_parts, sl->d_err);
     e = s->mixed ? eaf::launch_batch_mixed(tt, G, eaf::kBatchBlock, s->max_outer,
@@ -391,7 +419,7 @@ int eaf_srv_create(eaf_srv_t* out, int device, double hbm_budget_bytes, int mixe
   s->next_run = 1;
   s->next_ticket = 1;
   int rc = eaf::batch_capacity(device, &s->capacity);
-  cudaError_t e = cudaSuccess;
+  cudaError_t e = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
   const size_t tab_ints = (size_t)s->capacity * 4 + 2 + max_batch;
   for (SrvSlot& sl : s->slots) {
     if (e != cudaSuccess || rc != EAF_OK) break;

@@ -119,3 +119,30 @@ def test_campaign_client_stream():
                            seed=1, max_wall=120.0)
     assert st["solves"] == 3 * st["runs"] and st["runs"] > 0
     assert st["max_residual"] < 1e-8 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_large_run_is_solved_at_full_width_and_same_in_the_mix():
+    """A 60x120x84 run (over the large-run threshold) is solved over the whole
+    device with the single-system launch of its mesh: its warm-started
+    sequence equals the single-system solver's bit for bit, alone and beside
+    small runs, and the small runs still finish."""
+    eaf = pkg()
+    g = gen()
+    big = (60, 120, 84, 24)
+    rounds = 2
+    seq = sequence(big, 5, rounds)
+    ref = []
+    phi = g.zeros_phi(*big[:3])
+    with eaf.CGSolver(*big[:3]) as cg:
+        for s in seq:
+            res, nit, st = cg.solve(s.arrays(), phi, 200000, 1e-8)
+            assert st == 0
+            ref.append(phi.copy())
+    with eaf.Server() as srv:
+        runs = [(srv.open_run(*big[:3]), seq, g.zeros_phi(*big[:3]))]
+        for j, d in enumerate(OTHERS[:3]):
+            runs.append((srv.open_run(*d[:3]), sequence(d, 70 + j, rounds),
+                         g.zeros_phi(*d[:3])))
+        mix = solve_rounds(srv, runs, rounds)
+    for k in range(rounds):
+        assert np.array_equal(mix[0][k], ref[k]), f"round {k} differs"
