@@ -40,9 +40,14 @@ namespace eaf {
 namespace {
 
 // Shared-memory arrays of a slice, in this order:
-//   coefficients aP aW aE aS aN aB aT, then x r z p0 p1 q.
-constexpr int kDsmArrays = 13;
-enum { kAP, kAW, kAE, kAS, kAN, kAB, kAT, kX, kR, kZ, kP0, kP1, kQ };
+//   coefficients aP aW aE aS aN aB aT, then x r z p0 p1 q, then the six
+//   neighbour addresses of every cell (32-bit shared-window addresses of the
+//   neighbour's element of array 0 in its owner block, or kNoNeighbour at an
+//   r or z wall), which occupy the room of three more arrays.
+constexpr int kDsmArrays = 16;
+enum { kAP, kAW, kAE, kAS, kAN, kAB, kAT, kX, kR, kZ, kP0, kP1, kQ, kNB };
+enum { kW, kE, kS, kN, kB, kT };  // neighbour directions, stencil order
+constexpr uint32_t kNoNeighbour = 0xFFFFFFFFu;
 
 struct DsmArgs {
   MeshDims d;
@@ -98,13 +103,18 @@ struct Dsm {
   int chunk, rank;
   FastDiv fd;
   __device__ __forceinline__ double* arr(int k) const { return base + (size_t)k * chunk; }
-  // Value of array k at compact cell cc, wherever it lives in the cluster.
-  __device__ __forceinline__ double at(int k, int cc) const {
+  __device__ __forceinline__ uint32_t* nb(int dir) const {
+    return reinterpret_cast<uint32_t*>(base + (size_t)kNB * chunk) + (size_t)dir * chunk;
+  }
+  // Address (in the cluster's shared window) of array 0 at compact cell cc.
+  __device__ __forceinline__ uint32_t where(int cc) const {
     const int owner = (int)fd.div((uint32_t)cc);
     const int off = cc - owner * chunk;
-    if (owner == rank) return base[(size_t)k * chunk + off];
-    const uint32_t a = base_sa + 8u * (uint32_t)((size_t)k * chunk + off);
-    return ld_cluster_f64(cluster_map(a, (uint32_t)owner));
+    return cluster_map(base_sa + 8u * (uint32_t)off, (uint32_t)owner);
+  }
+  // Value of array k at the neighbour whose array-0 address is a.
+  __device__ __forceinline__ double at(int k, uint32_t a) const {
+    return ld_cluster_f64(a + 8u * (uint32_t)k * (uint32_t)chunk);
   }
 };
 
@@ -176,32 +186,31 @@ __device__ __forceinline__ bool dsm_allsum(double (&v)[NV], PartSmem& ps, Exchan
   return ok;
 }
 
-// y = A x at compact cell c (own), the reference's expression order; the
-// coefficients are this block's copies, x values come from xv(cell).
+// y = A x at own cell o, the reference's expression order; the coefficients
+// are this block's copies, neighbour values come from xv(neighbour address)
+// (a missing neighbour -- r or z wall -- is skipped in the symmetric form and
+// multiplies a zero value in the general form, as in apply_row_with).
 template <bool SYM, typename XF>
-__device__ __forceinline__ double dsm_row(const MeshDims& d, const Dsm& m, int o, int c,
-                                          double xc, XF xv) {
-  int i, j, k;
-  cell_ijk(d, c, i, j, k);
-  const int cs = j > 0 ? c - d.nr : c + (d.nth - 1) * d.nr;
-  const int cn = j < d.nth - 1 ? c + d.nr : c - (d.nth - 1) * d.nr;
+__device__ __forceinline__ double dsm_row(const Dsm& m, int o, double xc, XF xv) {
+  const uint32_t w = m.nb(kW)[o], e = m.nb(kE)[o], so = m.nb(kS)[o];
+  const uint32_t no = m.nb(kN)[o], bo = m.nb(kB)[o], t = m.nb(kT)[o];
   double y = m.arr(kAP)[o] * xc;
   if (SYM) {
-    if (i > 0) y = y - m.arr(kAW)[o] * xv(c - 1);
-    if (i < d.nr - 1) y = y - m.arr(kAE)[o] * xv(c + 1);
-    y = y - m.arr(kAS)[o] * xv(cs);
-    y = y - m.arr(kAN)[o] * xv(cn);
-    if (k > 0) y = y - m.arr(kAB)[o] * xv(c - d.plane);
-    if (k < d.nz - 1) y = y - m.arr(kAT)[o] * xv(c + d.plane);
+    if (w != kNoNeighbour) y = y - m.arr(kAW)[o] * xv(w);
+    if (e != kNoNeighbour) y = y - m.arr(kAE)[o] * xv(e);
+    y = y - m.arr(kAS)[o] * xv(so);
+    y = y - m.arr(kAN)[o] * xv(no);
+    if (bo != kNoNeighbour) y = y - m.arr(kAB)[o] * xv(bo);
+    if (t != kNoNeighbour) y = y - m.arr(kAT)[o] * xv(t);
   } else {
-    const double xw = i > 0 ? xv(c - 1) : 0.0;
-    const double xe = i < d.nr - 1 ? xv(c + 1) : 0.0;
-    const double xb = k > 0 ? xv(c - d.plane) : 0.0;
-    const double xt = k < d.nz - 1 ? xv(c + d.plane) : 0.0;
+    const double xw = w != kNoNeighbour ? xv(w) : 0.0;
+    const double xe = e != kNoNeighbour ? xv(e) : 0.0;
+    const double xb = bo != kNoNeighbour ? xv(bo) : 0.0;
+    const double xt = t != kNoNeighbour ? xv(t) : 0.0;
     y = y - m.arr(kAW)[o] * xw;
     y = y - m.arr(kAE)[o] * xe;
-    y = y - m.arr(kAS)[o] * xv(cs);
-    y = y - m.arr(kAN)[o] * xv(cn);
+    y = y - m.arr(kAS)[o] * xv(so);
+    y = y - m.arr(kAN)[o] * xv(no);
     y = y - m.arr(kAB)[o] * xb;
     y = y - m.arr(kAT)[o] * xt;
   }
@@ -246,6 +255,13 @@ __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
       m.arr(kAB)[o] = s.aB[c];
     }
     m.arr(kX)[o] = s.x[c];
+    const int cn = j < d.nth - 1 ? c + d.nr : c - (d.nth - 1) * d.nr;
+    m.nb(kW)[o] = i > 0 ? m.where(c - 1) : kNoNeighbour;
+    m.nb(kE)[o] = i < d.nr - 1 ? m.where(c + 1) : kNoNeighbour;
+    m.nb(kS)[o] = m.where(cs);
+    m.nb(kN)[o] = m.where(cn);
+    m.nb(kB)[o] = k > 0 ? m.where(c - d.plane) : kNoNeighbour;
+    m.nb(kT)[o] = k < d.nz - 1 ? m.where(c + d.plane) : kNoNeighbour;
   }
   // Preamble (src/mod_solver_3d.f90:515-530): ||Su||, z = r/max(|aP|,SMALL),
   // p = z, r.z and r.r.
@@ -279,23 +295,23 @@ __device__ void dsm_body(const DsmArgs& a, const Dsm& m, PartSmem& ps, int C) {
       double* q = m.arr(kQ);
       double v1[1] = {0.0};
       if (iter == 1) {
-        auto xv = [&m, kcur](int cc) { return m.at(kcur, cc); };
+        auto xv = [&m, kcur](uint32_t na) { return m.at(kcur, na); };
         for (int c = begin + (int)threadIdx.x; c < end; c += B) {
           const int o = c - begin;
           const double pc = pcur[o];
-          const double qv = dsm_row<SYM>(d, m, o, c, pc, xv);
+          const double qv = dsm_row<SYM>(m, o, pc, xv);
           q[o] = qv;
           v1[0] = v1[0] + pc * qv;
         }
       } else {
         const double bt = beta;
-        auto pnew = [&m, kold, bt](int cc) { return m.at(kZ, cc) + bt * m.at(kold, cc); };
+        auto pnew = [&m, kold, bt](uint32_t na) { return m.at(kZ, na) + bt * m.at(kold, na); };
         const double* z = m.arr(kZ);
         const double* pold = m.arr(kold);
         for (int c = begin + (int)threadIdx.x; c < end; c += B) {
           const int o = c - begin;
           const double pc = z[o] + bt * pold[o];
-          const double qv = dsm_row<SYM>(d, m, o, c, pc, pnew);
+          const double qv = dsm_row<SYM>(m, o, pc, pnew);
           pcur[o] = pc;
           q[o] = qv;
           v1[0] = v1[0] + pc * qv;
