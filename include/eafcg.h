@@ -533,13 +533,6 @@ int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device, void* stream,
  * intact. No reference counterpart (failure-detection test hook). */
 int eaf_selftest_barrier_timeout(int device, double timeout_ms);
 
-/* Diagnostics (no reference counterpart): device time of one group
- * all-reduce of two sums -- block reduction, bounded group barrier, staging
- * and fold of the block partials -- averaged over `iters` in one cooperative
- * launch of blocks x threads, in form 0, 1 or 2 (full block barriers around
- * a counter barrier with three memory-ordering variants) or 3 (warp 0
- * exchanges while the other warps wait once on a named barrier; the form
- * the solvers use). All forms fold in the same order. */
 /* Diagnostics (no reference counterpart): checks, on n generated operand
  * pairs (random over a wide exponent range, exact and near-halfway
  * quotients, zeros, infinities, NaN), that the division the TDMA sweeps use
@@ -548,6 +541,13 @@ int eaf_selftest_barrier_timeout(int device, double timeout_ms);
 int eaf_diag_div_check(int device, long long n, unsigned long long seed,
                        long long* mismatches, long long* fast_path);
 
+/* Diagnostics (no reference counterpart): device time of one group
+ * all-reduce of two sums -- block reduction, bounded group barrier, staging
+ * and fold of the block partials -- averaged over `iters` in one cooperative
+ * launch of blocks x threads, in form 0, 1 or 2 (full block barriers around
+ * a counter barrier with three memory-ordering variants) or 3 (warp 0
+ * exchanges while the other warps wait once on a named barrier; the form
+ * the solvers use). All forms fold in the same order. */
 int eaf_diag_allreduce_us(int device, int blocks, int threads, int iters,
                           int form, double* us_per_allreduce);
 
