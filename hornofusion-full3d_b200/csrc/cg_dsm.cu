@@ -20,7 +20,7 @@
 //     cluster all-reduce with one cluster (the oracle's plan (C, B, C)), so
 //     the solve is bit-identical to cg_cluster_kernel on the same launch
 //     shape and to the oracle. The signal is either a full cluster barrier
-//     (the default: measured faster, 3.6 against 4.1 us per iteration at
+//     (the default: measured faster, 3.4 against 3.9 us per iteration at
 //     12x24x16) or a remote arrival on an mbarrier of each block (release at
 //     cluster scope, one arrival per block and phase, barriers
 //     double-buffered by all-reduce parity).
