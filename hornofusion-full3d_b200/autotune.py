@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 MESHES = [(12, 24, 16, 8), (18, 36, 24, 8), (35, 70, 50, 16), (60, 120, 84, 24),
           (120, 240, 168, 64)]
 LATENCY_SLACK = 2.5
-RESIDENT_MAX_CELLS = 35000
+RESIDENT_MAX_CELLS = 28000
 
 
 def select(log):

@@ -109,7 +109,7 @@ int max_active_clusters(int block, long long n, int cluster);
 // The same solve on ONE cluster of `cluster` blocks whose shared memory holds
 // the whole system for the whole solve (cg_dsm.cu); bit-identical to the
 // cluster kernel on the launch (cluster, block, cluster). Meshes of at most
-// dsm_max_cells(cluster) cells (about 35,000 at 16 blocks on B200).
+// dsm_max_cells(cluster) cells (about 28,000 at 16 blocks on B200).
 // `signal` picks how a block signals its partials: kDsmSignalClusterBarrier
 // (a full cluster barrier, default: measured faster) or kDsmSignalMbarrier
 // (remote mbarrier arrivals).

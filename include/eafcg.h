@@ -150,7 +150,7 @@ int eaf_cg_get_cluster(eaf_cg_t h, int* cluster_blocks);
 int eaf_cg_last_cluster(eaf_cg_t h, int* cluster_blocks);
 
 /* A launch that is ONE cluster (grid == cluster blocks) on a mesh that fits
- * the cluster's shared memory (about 35,000 cells at 16 blocks) runs, by
+ * the cluster's shared memory (about 28,000 cells at 16 blocks) runs, by
  * default, the cluster-resident kernel: the whole system lives in
  * distributed shared memory for the whole solve and an iteration touches no
  * global memory. resident = 1: its blocks signal their partials by a full
