@@ -47,6 +47,8 @@ def lib():
         L.eaf_oracle_cg1.restype = ci
         L.eaf_oracle_dot.argtypes = [ci, ci, ci, _dp, _dp, ci, ci]
         L.eaf_oracle_dot.restype = cd
+        L.eaf_oracle_dot_cluster.argtypes = [ci, ci, ci, _dp, _dp, ci, ci, ci]
+        L.eaf_oracle_dot_cluster.restype = cd
         L.eaf_oracle_matvec.argtypes = [ci, ci, ci] + [_dp] * 9
         L.eaf_oracle_matvec.restype = None
         L.eaf_oracle_theta_wrap.argtypes = [ci, ci, ci, _dp]
@@ -127,7 +129,13 @@ def matvec(system, x: np.ndarray) -> np.ndarray:
 
 def dot(nr: int, nth: int, nz: int, a: np.ndarray, b: np.ndarray,
         plan: tuple | None = None) -> float:
-    G, B = plan if plan is not None else (0, 0)
+    """Interior dot in the association of ``plan`` ((G, B) or (G, B, C));
+    the reference's sequential sum without one."""
+    if plan is not None and len(plan) > 2 and int(plan[2]) > 1:
+        G, B, C = plan
+        return lib().eaf_oracle_dot_cluster(nr, nth, nz, _p(a), _p(b), int(G), int(B),
+                                            int(C))
+    G, B = plan[:2] if plan is not None else (0, 0)
     return lib().eaf_oracle_dot(nr, nth, nz, _p(a), _p(b), int(G), int(B))
 
 

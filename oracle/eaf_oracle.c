@@ -529,6 +529,20 @@ double eaf_oracle_dot(int nr, int nth, int nz, const double* a, const double* b,
     return dot(&o, a, b);
 }
 
+/* The same on a grid of thread-block clusters of C blocks (G a multiple of
+ * C): the association of the cluster all-reduce (see dot_tree). */
+double eaf_oracle_dot_cluster(int nr, int nth, int nz, const double* a, const double* b,
+                              int G, int B, int C) {
+    op_t o;
+    memset(&o, 0, sizeof(o));
+    o.d = mkdims(nr, nth, nz);
+    o.nthreads = 1;
+    o.plan.G = G;
+    o.plan.B = B;
+    o.plan.C = C;
+    return dot(&o, a, b);
+}
+
 /* Threaded variant (OpenMP over k-planes) used only as the timed CPU
  * baseline: same algorithm and guards, plane-partial dots. */
 int eaf_oracle_cg_threads(int nr, int nth, int nz, const double* aW,

@@ -238,8 +238,11 @@ def test_max_iter_zero(orc):
     assert not g.interior(phi).any()
 
 
-def py_tree_dot(a, b, G, B):
-    """Pure-Python model of the CUDA reduction tree (cg_common.cuh)."""
+def py_tree_dot(a, b, G, B, C=1):
+    """Pure-Python model of the CUDA reduction tree (cg_common.cuh) and, with
+    C > 1, of the cluster all-reduce (cluster_red.cuh): block partials of a
+    cluster folded in rank order from the first, the cluster partials in
+    place of the block partials in the last stage."""
     prod = (a * b).ravel()
     n = prod.size
     chunk = -(-n // G)
@@ -264,7 +267,15 @@ def py_tree_dot(a, b, G, B):
         ws = [bfly([lanes[w * 32 + l] if w * 32 + l < B else 0.0 for l in range(32)])
               for w in range(nw)]
         parts.append(bfly(ws + [0.0] * (32 - nw)))
-    if G == 1:
+    if C > 1:
+        cps = []
+        for c0 in range(0, G, C):
+            cp = parts[c0]
+            for r in range(1, C):
+                cp = cp + parts[c0 + r]
+            cps.append(cp)
+        parts = cps
+    if len(parts) == 1:
         return parts[0]
     return bfly([sum_seq(parts[l::32]) for l in range(32)])
 
@@ -286,6 +297,30 @@ def test_kernel_order_dot_matches_python_model(orc, plan):
     want = py_tree_dot(g.interior(a), g.interior(b), *plan)
     assert got == want
     assert abs(got - orc.dot(12, 24, 16, a, b)) < 1e-9
+
+
+@pytest.mark.parametrize("plan", [(16, 288, 16), (8, 64, 2), (40, 32, 4), (148, 32, 4),
+                                  (150, 32, 2), (16, 128, 1)])
+def test_cluster_plan_dot_matches_python_model(orc, plan):
+    """The oracle's cluster association (one cluster, several, more than 32
+    and more than 64 clusters) against the Python model; C = 1 is the flat
+    association."""
+    g = gen()
+    rng = np.random.default_rng(10)
+    a = rng.normal(size=g.halo_shape(12, 24, 16))
+    b = rng.normal(size=a.shape)
+    got = orc.dot(12, 24, 16, a, b, plan)
+    assert got == py_tree_dot(g.interior(a), g.interior(b), *plan)
+    if plan[2] == 1:
+        assert got == orc.dot(12, 24, 16, a, b, plan[:2])
+
+
+def test_cluster_plan_of_one_block_clusters_equals_flat_plan(orc):
+    g = gen()
+    s = g.make_system(*g.SMOKE, seed=0)
+    p1, p2 = g.zeros_phi(12, 24, 16), g.zeros_phi(12, 24, 16)
+    assert orc.cg(s, p1, 200, 0.0, plan=(9, 256)) == orc.cg(s, p2, 200, 0.0, plan=(9, 256, 1))
+    assert np.array_equal(p1, p2)
 
 
 def test_kernel_order_solve_agrees_with_sequential_closely(orc):
