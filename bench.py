@@ -1024,7 +1024,7 @@ def run_fixed(args):
                 cg.set_cluster(args.cluster)
             if args.kernel is not None:
                 cg.set_kernel({"loads": cg.KERNEL_LOADS, "stream": cg.KERNEL_STREAM,
-                               "slots": cg.KERNEL_SLOTS}[args.kernel])
+                               "slots": cg.KERNEL_SLOTS, "keep": cg.KERNEL_KEEP}[args.kernel])
             for _ in range(args.repeat):
                 phi.zero_()
                 torch.cuda.synchronize()
@@ -1039,8 +1039,9 @@ def run_fixed(args):
                              "kernel_ms": t["kernel_ms"], "solve_ms": t["solve_ms"],
                              "us_per_iter": 1e3 * t["kernel_ms"] / max(nit, 1)})
             launch = list(cg.last_launch())
+            kernel = cg.last_kernel()
         case = {"mesh": [nr, nth, nz], "iters": args.iters, "mixed": args.mixed,
-                "cg_form": args.cg_form}
+                "cg_form": args.cg_form, "flat_kernel": kernel}
     print(json.dumps({"workload": "fixed", "case": case, "launch": launch, "runs": runs}),
           flush=True)
     return 0
@@ -1095,7 +1096,7 @@ def main(argv=None):
     ap.add_argument("--launch", type=int, nargs=2, default=None, metavar=("BLOCK", "GRID"))
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--batch-size", type=int, default=0)
-    ap.add_argument("--kernel", choices=["loads", "stream", "slots"], default=None,
+    ap.add_argument("--kernel", choices=["loads", "stream", "slots", "keep"], default=None,
                     help="FP64 kernel on a flat grid (default: the tuned choice)")
     ap.add_argument("--fixed-tdma", action="store_true")
     args = ap.parse_args(argv)

@@ -297,12 +297,15 @@ class CGSolver:
     KERNEL_LOADS = 1
     KERNEL_STREAM = 2
     KERNEL_SLOTS = 3
+    KERNEL_KEEP = 4
 
     def set_kernel(self, kernel: int = 0) -> None:
         """Kernel of the plain FP64 solve on a flat grid: KERNEL_LOADS
         (per-thread loads), KERNEL_STREAM (bulk-copy staging), KERNEL_SLOTS
-        (per-thread loads, slot-polling all-reduce) or KERNEL_AUTO (the tuned
-        choice); the same bits either way."""
+        (per-thread loads, slot-polling all-reduce), KERNEL_KEEP (own cells'
+        update operands kept in shared memory; where a block's slice does not
+        fit, per-thread loads run) or KERNEL_AUTO (the tuned choice); the
+        same bits either way."""
         check(self._lib.eaf_cg_set_kernel(self._h, int(kernel)), "set_kernel")
 
     def last_kernel(self) -> int:

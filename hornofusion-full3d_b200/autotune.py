@@ -7,7 +7,9 @@ counts (tol 0) and CUDA-event device times from the library:
 
 * single-system solver (eaf_cg_*): the time per iteration of the persistent
   kernel for block sizes 256/512/1024 and grid sizes from one block up to
-  the co-resident maximum, and, on meshes that fit one cluster's shared
+  the co-resident maximum, with per-thread loads and, where a block's slice
+  fits its shared memory, with the update operands kept there; the
+  bulk-copy streaming kernel on one block per SM; and, on meshes that fit one cluster's shared
   memory, the cluster-resident kernel on one cluster of 4, 8 or 16 blocks of
   128 to 1024 threads; the fastest (block, grid, cluster) is kept;
 * batched/served solver (eaf_batch_*): the time per iteration t(w) of one
@@ -37,6 +39,7 @@ MESHES = [(12, 24, 16, 8), (18, 36, 24, 8), (35, 70, 50, 16), (60, 120, 84, 24),
           (120, 240, 168, 64)]
 LATENCY_SLACK = 2.5
 RESIDENT_MAX_CELLS = 28000
+KEEP_MAX_SLICE_BYTES = 220 * 1024  # kept operands of one block's slice
 
 
 def select(log):
@@ -62,16 +65,25 @@ def select(log):
     return single, lanes
 
 
-def time_single(eaf, dev_arrays, phi, dims, block, grid, iters, cluster=1, stream=0):
+# Flat-grid kernel codes of the table: per-thread loads, bulk-copy
+# streaming, own cells kept in shared memory.
+FLAT_LOADS, FLAT_STREAM, FLAT_KEEP = 0, 1, 2
+
+
+def time_single(eaf, dev_arrays, phi, dims, block, grid, iters, cluster=1, stream=FLAT_LOADS,
+                want_kernel=False):
     with eaf.CGSolver(*dims) as cg:
         cg.set_launch(block, grid)
         cg.set_cluster(cluster)
-        cg.set_kernel(cg.KERNEL_STREAM if stream else cg.KERNEL_LOADS)
+        cg.set_kernel({FLAT_LOADS: cg.KERNEL_LOADS, FLAT_STREAM: cg.KERNEL_STREAM,
+                       FLAT_KEEP: cg.KERNEL_KEEP}[stream])
         best = float("inf")
         for _ in range(2):
             phi.zero_()
             cg.solve(dev_arrays, phi, iters, 0.0, device_ptrs=True)
             best = min(best, cg.last_timing()["kernel_ms"] / iters)
+        if want_kernel:
+            return best * 1e3, cg.last_launch(), cg.last_kernel() == cg.KERNEL_KEEP
         return best * 1e3, cg.last_launch()
 
 
@@ -134,10 +146,17 @@ def main(argv=None) -> int:
             us, used = time_single(eaf, dev, phi, dims, block, grid, args.iters)
             log.append({"mesh": dims, "solver": "single", "block": block, "grid": used[0],
                         "us_per_iter": round(us, 3)})
+            if 5 * 8 * math.ceil(n / grid) <= KEEP_MAX_SLICE_BYTES:
+                us, used, kept = time_single(eaf, dev, phi, dims, block, grid, args.iters,
+                                             1, FLAT_KEEP, want_kernel=True)
+                if kept:
+                    log.append({"mesh": dims, "solver": "single", "block": block,
+                                "grid": used[0], "stream": FLAT_KEEP,
+                                "us_per_iter": round(us, 3)})
         for block in (512, 1024):  # the bulk-copy streaming kernel, one block per SM
-            us, used = time_single(eaf, dev, phi, dims, block, sms, args.iters, 1, 1)
+            us, used = time_single(eaf, dev, phi, dims, block, sms, args.iters, 1, FLAT_STREAM)
             log.append({"mesh": dims, "solver": "single", "block": block, "grid": used[0],
-                        "stream": 1, "us_per_iter": round(us, 3)})
+                        "stream": FLAT_STREAM, "us_per_iter": round(us, 3)})
         if n <= RESIDENT_MAX_CELLS:  # one cluster holding the system on chip
             for c in (4, 8, 16):
                 for block in (128, 256, 288, 512, 1024):
@@ -206,8 +225,9 @@ struct TunedLaunch {{
   int nr, nth, nz, block, grid, cluster, stream;
 }};
 
-// (block, grid, blocks per cluster (1 = no clusters), bulk-copy streaming
-// kernel (1) or per-thread loads (0)) of the single-system persistent solver.
+// (block, grid, blocks per cluster (1 = no clusters), flat-grid kernel:
+// per-thread loads (0), bulk-copy streaming (1) or own cells kept in shared
+// memory (2)) of the single-system persistent solver.
 static constexpr TunedLaunch kTunedLaunches[] = {{
 {rows_s}
 }};

@@ -164,13 +164,17 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
       }
     }
   }
-  int stream = 0, slots = 0;
-  if (f64 && form == EAF_CG_FORM_REFERENCE && c == 1 && req_kernel == EAF_CG_KERNEL_SLOTS)
-    slots = 1;
-  if (f64 && form == EAF_CG_FORM_REFERENCE && c == 1 && !slots) {
-    stream = req_kernel == EAF_CG_KERNEL_STREAM ? 1
-             : req_kernel == EAF_CG_KERNEL_LOADS ? 0
-                                                 : (automatic ? ts : 0);
+  int stream = 0, slots = 0, keep = 0;
+  if (f64 && form == EAF_CG_FORM_REFERENCE && c == 1) {
+    int k = req_kernel;
+    if (k == EAF_CG_KERNEL_AUTO)
+      k = !automatic ? EAF_CG_KERNEL_LOADS
+          : ts == 2  ? EAF_CG_KERNEL_KEEP
+          : ts == 1  ? EAF_CG_KERNEL_STREAM
+                     : EAF_CG_KERNEL_LOADS;
+    slots = k == EAF_CG_KERNEL_SLOTS;
+    stream = k == EAF_CG_KERNEL_STREAM;
+    keep = k == EAF_CG_KERNEL_KEEP;
     if (stream && (b % 32 != 0 || stream_max_coresident(b, nr, sms) < 1)) stream = 0;
   }
   if (c == 1) {
@@ -179,12 +183,16 @@ SolverLaunch choose_launch(int nr, int nth, int nz, int sms, int req_block, int 
     if (cap > 0 && g > cap) g = cap;
     if (g > sms * 8) g = sms * 8;
   }
+  // The kept slices must fit the shared memory of blocks that are all
+  // resident at once; otherwise the per-thread-load kernel runs.
+  if (keep && keep_max_coresident(b, n, g, sms) < g) keep = 0;
   SolverLaunch L;
   L.grid = g;
   L.block = b;
   L.cluster = c;
   L.stream = stream;
   L.slots = slots;
+  L.keep = keep;
   if (slots && g > kMaxClusters) L.grid = kMaxClusters;
   return L;
 }
@@ -206,6 +214,8 @@ cudaError_t launch_f64_solver(const SolverLaunch& L, int resident, const MeshDim
                                  L.grid, L.block, L.cluster, st);
   if (L.stream)
     return launch_cg_f64_stream(d, s, ws, max_iter, tol, timeout_ns, L.grid, L.block, st);
+  if (L.keep)
+    return launch_cg_f64_keep(d, s, ws, max_iter, tol, timeout_ns, L.grid, L.block, st);
   return launch_cg_f64(d, s, ws, max_iter, tol, timeout_ns, L.grid, L.block, st);
 }
 
@@ -372,15 +382,17 @@ int eaf_cg_mixed_trace(eaf_cg_t h, double* steps, int max_steps, int* n_steps) {
 }
 
 int eaf_cg_set_kernel(eaf_cg_t h, int kernel) {
-  if (!h || kernel < EAF_CG_KERNEL_AUTO || kernel > EAF_CG_KERNEL_SLOTS) return EAF_EINVAL;
+  if (!h || kernel < EAF_CG_KERNEL_AUTO || kernel > EAF_CG_KERNEL_KEEP) return EAF_EINVAL;
   h->kernel = kernel;
   return EAF_OK;
 }
 
 int eaf_cg_last_kernel(eaf_cg_t h, int* kernel) {
   if (!h || !kernel) return EAF_EINVAL;
-  *kernel = h->last_stream == 2 ? EAF_CG_KERNEL_SLOTS
-            : h->last_stream ? EAF_CG_KERNEL_STREAM : EAF_CG_KERNEL_LOADS;
+  *kernel = h->last_stream == 3   ? EAF_CG_KERNEL_KEEP
+            : h->last_stream == 2 ? EAF_CG_KERNEL_SLOTS
+            : h->last_stream      ? EAF_CG_KERNEL_STREAM
+                                  : EAF_CG_KERNEL_LOADS;
   return EAF_OK;
 }
 
@@ -505,7 +517,7 @@ int enqueue_solve(eaf_cg* h, const HaloInputs& in, double* phi, const SolveOpts&
                                   h->st, h->trace_d));
   } else {
     const eaf::SolverLaunch L = pick_launch(h, true, &grid, &block, &cluster);
-    h->last_stream = L.slots ? 2 : L.stream;
+    h->last_stream = L.keep ? 3 : L.slots ? 2 : L.stream;
     EAF_CUDA(cudaEventRecord(h->ev[2], h->st));
     if (h->form == EAF_CG_FORM_ONE_REDUCTION)
       EAF_CUDA(eaf::launch_cg1_f64(h->d, h->s, h->ws, o.max_iter, o.tol, h->timeout_ns,

@@ -89,11 +89,24 @@ struct CgArgs {
 // phase. Kernels pick them by their register budget. PF: threads 0..7 of the
 // block prefetch the block's next round of every streamed array into L2
 // (one bulk prefetch per array), for meshes whose working set exceeds L2.
-template <bool SYM, int U, int UA, bool PF, class G>
-__device__ void cg_body(const CgArgs& a, G& g) {
+// KEEP: the thread's own cells' x, r, aP and this iteration's p and q stay
+// in the block's shared memory (`keep`, 5 x slice-length doubles) for the
+// whole solve: the update phase then reads no global memory, q is never
+// stored globally, and x goes back to global memory once, at the end. A
+// thread visits the same cells in both phases (and every iteration), so no
+// other thread ever reads what it keeps; the arithmetic and the order of
+// every sum are unchanged.
+template <bool SYM, int U, int UA, bool PF, class G, bool KEEP = false>
+__device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
   const MeshDims& d = a.d;
   const SysF64& s = a.s;
   const Slice own = own_slice(d.n, g.nb, g.bid);
+  const int slen = own.end - own.begin;
+  double* __restrict__ kx = keep;
+  double* __restrict__ kr = keep + (size_t)1 * (KEEP ? slen : 0);
+  double* __restrict__ kd = keep + (size_t)2 * (KEEP ? slen : 0);
+  double* __restrict__ kp = keep + (size_t)3 * (KEEP ? slen : 0);
+  double* __restrict__ kq = keep + (size_t)4 * (KEEP ? slen : 0);
   const Coefs<double> A = coefs_of<double>(s.aP, s.aE, s.aN, s.aT, s.aW, s.aS, s.aB);
   const double* __restrict__ aP = s.aP;
   const double* __restrict__ b = s.b;
@@ -123,6 +136,13 @@ __device__ void cg_body(const CgArgs& a, G& g) {
         const bool live = c0 + u * B < own.end;
         const double zv = rv[u] / guard_small(fabs(dv[u]));
         if (live) p0[c0 + u * B] = zv;
+        if (KEEP && live) {
+          const int o = c0 + u * B - own.begin;
+          kx[o] = x[c0 + u * B];
+          kr[o] = rv[u];
+          kd[o] = dv[u];
+          kp[o] = zv;
+        }
         v3[0] = v3[0] + (live ? bv[u] * bv[u] : 0.0);
         v3[1] = v3[1] + (live ? rv[u] * rv[u] : 0.0);
         v3[2] = v3[2] + (live ? rv[u] * zv : 0.0);
@@ -167,7 +187,12 @@ __device__ void cg_body(const CgArgs& a, G& g) {
 #pragma unroll
           for (int u = 0; u < UA; ++u) {
             const bool live = c0 + u * B < own.end;
-            if (live) q[c0 + u * B] = qv[u];
+            if (live) {
+              if (KEEP)
+                kq[c0 + u * B - own.begin] = qv[u];
+              else
+                q[c0 + u * B] = qv[u];
+            }
             v1[0] = v1[0] + (live ? pc[u] * qv[u] : 0.0);
           }
         }
@@ -193,7 +218,12 @@ __device__ void cg_body(const CgArgs& a, G& g) {
             const bool live = c0 + u * B < own.end;
             if (live) {
               pcur[c0 + u * B] = pc[u];
-              q[c0 + u * B] = qv[u];
+              if (KEEP) {
+                kp[c0 + u * B - own.begin] = pc[u];
+                kq[c0 + u * B - own.begin] = qv[u];
+              } else {
+                q[c0 + u * B] = qv[u];
+              }
             }
             v1[0] = v1[0] + (live ? pc[u] * qv[u] : 0.0);
           }
@@ -215,11 +245,20 @@ __device__ void cg_body(const CgArgs& a, G& g) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int c = min(c0 + u * B, last);
-          pv[u] = pcur[c];
-          qv[u] = q[c];
-          dv[u] = aP[c];
-          xv[u] = x[c];
-          rv[u] = r[c];
+          if (KEEP) {
+            const int o = c - own.begin;
+            pv[u] = kp[o];
+            qv[u] = kq[o];
+            dv[u] = kd[o];
+            xv[u] = kx[o];
+            rv[u] = kr[o];
+          } else {
+            pv[u] = pcur[c];
+            qv[u] = q[c];
+            dv[u] = aP[c];
+            xv[u] = x[c];
+            rv[u] = r[c];
+          }
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -229,8 +268,13 @@ __device__ void cg_body(const CgArgs& a, G& g) {
           const double zv = rn / guard_small(fabs(dv[u]));
           if (live) {
             const int c = c0 + u * B;
-            x[c] = xn;
-            r[c] = rn;
+            if (KEEP) {
+              kx[c - own.begin] = xn;
+              kr[c - own.begin] = rn;
+            } else {
+              x[c] = xn;
+              r[c] = rn;
+            }
             z[c] = zv;
           }
           v2[0] = v2[0] + (live ? rn * rn : 0.0);
@@ -247,6 +291,9 @@ __device__ void cg_body(const CgArgs& a, G& g) {
       if (residual != residual && iter < a.max_iter) { nan_fill = true; break; }
       beta = v2[1] / guard_small(rz);
       rz = v2[1];
+    }
+    if (KEEP && !nan_fill) {  // the kept x back to global memory
+      for (int c = own.begin + (int)threadIdx.x; c < own.end; c += B) x[c] = kx[c - own.begin];
     }
     if (nan_fill) {
       const double qnan = __longlong_as_double(0x7ff8000000000000ll);
@@ -287,6 +334,26 @@ __global__ void __launch_bounds__(MAXB, 1) cg_f64_kernel(CgArgs a) {
     cg_body<true, U, UA, PF>(a, g);
   else
     cg_body<false, U, UA, PF>(a, g);
+}
+
+// The same solver with the own cells' update operands kept in shared memory
+// (cg_body's KEEP); blocks own at most kKeepMaxSlice cells.
+template <int MAXB, int U, int UA>
+__global__ void __launch_bounds__(MAXB, 1) cg_keep_kernel(CgArgs a) {
+  extern __shared__ __align__(16) double keep_smem[];
+  Group g;
+  g.counter = a.ws.counter;
+  g.err = a.ws.err;
+  g.part = a.ws.part;
+  g.stage = group_stage_smem();
+  g.nb = gridDim.x;
+  g.bid = blockIdx.x;
+  g.timeout_ns = a.timeout_ns;
+  g.epoch = 0;
+  if (*a.s.asym == 0)
+    cg_body<true, U, UA, false, Group, true>(a, g, keep_smem);
+  else
+    cg_body<false, U, UA, false, Group, true>(a, g, keep_smem);
 }
 
 // The same solver on a grid of thread-block clusters (cluster_red.cuh): the
@@ -1216,6 +1283,60 @@ cudaError_t launch_cg_f64_stream(const MeshDims& d, const SysF64& s, const Group
   if (e != cudaSuccess) return e;
   int stages = S;
   void* args[] = {&a, &stages};
+  return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(block), args, smem, st);
+}
+
+static const void* cg_keep_kernel_ptr(int block) {
+  if (block <= 256) return (const void*)cg_keep_kernel<256, 4, 4>;
+  if (block <= 512) return (const void*)cg_keep_kernel<512, 4, 2>;
+  return (const void*)cg_keep_kernel<1024, 2, 1>;
+}
+
+size_t keep_smem_bytes(long long n, int grid) {
+  const long long chunk = (n + grid - 1) / grid;
+  return (size_t)chunk * 5 * sizeof(double);
+}
+
+int keep_max_coresident(int block, long long n, int grid, int sms) {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+          cudaSuccess)
+    return 0;
+  const size_t smem = keep_smem_bytes(n, grid);
+  if (smem + 8 * 1024 > (size_t)optin) return 0;  // static shared memory and slack
+  const void* k = cg_keep_kernel_ptr(block);
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return per_sm * sms;
+}
+
+cudaError_t launch_cg_f64_keep(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                               int max_iter, double tol, uint64_t timeout_ns, int grid,
+                               int block, cudaStream_t st) {
+  CgArgs a;
+  a.d = d;
+  a.s = s;
+  a.ws = ws;
+  a.max_iter = max_iter;
+  a.tol = tol;
+  a.timeout_ns = timeout_ns;
+  const void* k = cg_keep_kernel_ptr(block);
+  const size_t smem = keep_smem_bytes(d.n, grid);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  void* args[] = {&a};
   return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(block), args, smem, st);
 }
 

@@ -93,6 +93,16 @@ cudaError_t launch_cg_f64_stream(const MeshDims& d, const SysF64& s, const Group
                                  int block, cudaStream_t st);
 int stream_stages(int block, int nr);
 int stream_max_coresident(int block, int nr, int sms);
+// The same solver with each block's own cells' x, r, aP, p and q kept in
+// its shared memory for the whole solve (5 doubles a cell, dynamic shared
+// memory of keep_smem_bytes); bit-identical to cg_f64_kernel on the same
+// launch. keep_max_coresident: blocks of that launch the device can hold at
+// once (0: the slice does not fit).
+cudaError_t launch_cg_f64_keep(const MeshDims& d, const SysF64& s, const GroupWs& ws,
+                               int max_iter, double tol, uint64_t timeout_ns, int grid,
+                               int block, cudaStream_t st);
+size_t keep_smem_bytes(long long n, int grid);
+int keep_max_coresident(int block, long long n, int grid, int sms);
 // The same solver on a grid of thread-block clusters of `cluster` blocks
 // (2..16; grid a multiple of it, at most 128 clusters): its all-reduces fold
 // through the leader block's shared memory in each cluster and a global
@@ -130,6 +140,7 @@ struct SolverLaunch {
   int grid, block, cluster;
   int stream = 0;  // 1: the bulk-copy streaming kernel (flat grids only)
   int slots = 0;   // 1: flat grid, slot-polling all-reduce (clusters of one)
+  int keep = 0;    // 1: flat grid, own cells kept in shared memory
 };
 // The launch a handle with the requested shape (0 = automatic) uses on an
 // nr x nth x nz mesh (api.cu): the tuned shape, else the fallback rules,

@@ -25,7 +25,7 @@ struct eaf_cg {
   int cluster;         // blocks per thread-block cluster; 0 = automatic, 1 = none
   int resident;        // one-cluster launches keep the system in shared memory
   int kernel;          // EAF_CG_KERNEL_*: per-thread loads or bulk-copy streaming
-  int last_stream;     // the last FP64 solve's flat kernel: 0 loads, 1 stream, 2 slots
+  int last_stream;     // the last FP64 solve's flat kernel: 0 loads, 1 stream, 2 slots, 3 keep
   double* trace_d;     // mixed form: per refinement step trace (lazy)
   int trace_cap;       // refinement steps trace_d holds
   int sms;

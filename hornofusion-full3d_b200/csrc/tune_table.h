@@ -29,8 +29,9 @@ struct TunedLaunch {
   int nr, nth, nz, block, grid, cluster, stream;
 };
 
-// (block, grid, blocks per cluster (1 = no clusters), bulk-copy streaming
-// kernel (1) or per-thread loads (0)) of the single-system persistent solver.
+// (block, grid, blocks per cluster (1 = no clusters), flat-grid kernel:
+// per-thread loads (0), bulk-copy streaming (1) or own cells kept in shared
+// memory (2)) of the single-system persistent solver.
 static constexpr TunedLaunch kTunedLaunches[] = {
     {12, 24, 16, 288, 16, 16, 0},
     {18, 36, 24, 512, 16, 16, 0},

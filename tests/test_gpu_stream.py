@@ -107,7 +107,7 @@ def test_kernel_setting_is_validated():
     eaf = pkg()
     with eaf.CGSolver(12, 24, 16) as cg:
         with pytest.raises(eaf.EafError):
-            cg.set_kernel(4)
+            cg.set_kernel(5)
         with pytest.raises(eaf.EafError):
             cg.set_kernel(-1)
 
