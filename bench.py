@@ -80,13 +80,27 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch():
+def solver_kernel_name(solver, plan):
+    """Name of the persistent kernel the last solve of `solver` ran."""
+    if len(plan) > 2:
+        return "cg_dsm_kernel" if plan[0] == plan[2] else "cg_cluster_kernel"
+    return {solver.KERNEL_LOADS: "cg_f64_kernel", solver.KERNEL_STREAM: "cg_stream_kernel",
+            solver.KERNEL_SLOTS: "cg_cluster_kernel",
+            solver.KERNEL_KEEP: "cg_keep_kernel"}[solver.last_kernel()]
+
+
+def traffic_profile(kernel):
+    return os.path.join("profiles", f"{kernel}_60x120x84.txt")
+
+
+def ncu_traffic_per_launch(kernel):
     """DRAM bytes of one solver launch of this workload (a warm-started
-    re-solve), from the committed ncu summary, or None when no capture has
-    been summarised yet. The working set stays in L2 for the whole solve, so
-    a launch's traffic is its first read of the system plus the final write
-    and does not grow with its iterations; it is reported as captured."""
-    path = os.path.join(ROOT, "profiles", "cg_f64_kernel_60x120x84.txt")
+    re-solve), from the committed ncu summary of that kernel, or None when
+    no capture has been summarised yet. The working set stays in L2 for the
+    whole solve, so a launch's traffic is its first read of the system plus
+    the final write and does not grow with its iterations; it is reported
+    as captured."""
+    path = os.path.join(ROOT, traffic_profile(kernel))
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -287,6 +301,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     clk = clocks.stop()
     plan = solver.last_launch()
+    kernel = solver_kernel_name(solver, plan)
     if dist is not None:
         dist.barrier()
 
@@ -331,7 +346,7 @@ def run_ours(args, rank, world, local_rank):
     per_rank_ci = n * sum(iters)
     achieved = BYTES_PER_CELL_ITER * per_rank_ci / (kern_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic_per_launch()
+    traffic = ncu_traffic_per_launch(kernel)
     cpu = cpu_baseline_sample(g, seed=0) if world == 1 else None
     line = {
         "metric": METRIC, "value": value, "unit": "cell-iters/s", "n_gpus": world,
@@ -353,9 +368,8 @@ def run_ours(args, rank, world, local_rank):
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read+write of one bench "
-                                       "launch (profiles/cg_f64_kernel_60x120x84.txt)",
-                     "kernel": ("cg_cluster_kernel" if len(plan) > 2 else "cg_f64_kernel")
-                               + " (persistent, one launch per solve)",
+                                       f"launch ({traffic_profile(kernel)})",
+                     "kernel": kernel + " (persistent, one launch per solve)",
                      "algorithmic_bytes_per_cell_iter": BYTES_PER_CELL_ITER},
         "cpu_baseline": ({k: v for k, v in cpu.items() if k != "seconds"}
                          if cpu else None),

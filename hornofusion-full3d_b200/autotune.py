@@ -146,7 +146,7 @@ def main(argv=None) -> int:
             us, used = time_single(eaf, dev, phi, dims, block, grid, args.iters)
             log.append({"mesh": dims, "solver": "single", "block": block, "grid": used[0],
                         "us_per_iter": round(us, 3)})
-            if 5 * 8 * math.ceil(n / grid) <= KEEP_MAX_SLICE_BYTES:
+            if 4 * 8 * math.ceil(n / grid) <= KEEP_MAX_SLICE_BYTES:
                 us, used, kept = time_single(eaf, dev, phi, dims, block, grid, args.iters,
                                              1, FLAT_KEEP, want_kernel=True)
                 if kept:

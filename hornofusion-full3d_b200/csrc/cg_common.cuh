@@ -284,26 +284,52 @@ __device__ __forceinline__ bool group_allsum_w0(T (&v)[NV], Group& g, int slot) 
     // bar.warp.sync orders the other lanes' loads after lane 0's acquire.
     __syncwarp();
     ok = __shfl_sync(0xffffffffu, ok, 0);
-    // All of this lane's partials in one round of independent loads (groups
-    // of up to kMaxGroupBlocks / 32 = 37 per sum), then the fixed-order fold.
-    constexpr int kPer = 8;
+    // Lane l folds the partials of blocks l, l + 32, ... sequentially from
+    // 0.0, then the 32 lane sums are folded by the xor butterfly. Up to
+    // 32 * kFew blocks, every partial of every sum is loaded in one round of
+    // independent loads (one L2 round trip for all NV sums); larger groups
+    // load kPer partials per lane and sum at a time.
+    constexpr int kFew = 5;
+    if (g.nb <= 32 * kFew) {
+      double t[NV][kFew];
 #pragma unroll
-    for (int m = 0; m < NV; ++m) {
-      const double* p = g.part + (size_t)(slot + m) * g.nb;
-      double sum = 0.0;
-      for (int b0 = lane; b0 < g.nb; b0 += 32 * kPer) {
-        double t[kPer];
+      for (int m = 0; m < NV; ++m) {
+        const double* p = g.part + (size_t)(slot + m) * g.nb;
 #pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-          const int b = b0 + 32 * u;
-          t[u] = b < g.nb ? __ldcg(p + b) : 0.0;
+        for (int u = 0; u < kFew; ++u) {
+          const int b = lane + 32 * u;
+          t[m][u] = b < g.nb ? __ldcg(p + b) : 0.0;
         }
-#pragma unroll
-        for (int u = 0; u < kPer; ++u)
-          if (b0 + 32 * u < g.nb) sum = sum + t[u];
       }
-      sum = warp_allsum(sum);
-      if (lane == 0) s_tot[m] = sum;
+#pragma unroll
+      for (int m = 0; m < NV; ++m) {
+        double sum = 0.0;
+#pragma unroll
+        for (int u = 0; u < kFew; ++u)
+          if (lane + 32 * u < g.nb) sum = sum + t[m][u];
+        sum = warp_allsum(sum);
+        if (lane == 0) s_tot[m] = sum;
+      }
+    } else {
+      constexpr int kPer = 8;
+#pragma unroll
+      for (int m = 0; m < NV; ++m) {
+        const double* p = g.part + (size_t)(slot + m) * g.nb;
+        double sum = 0.0;
+        for (int b0 = lane; b0 < g.nb; b0 += 32 * kPer) {
+          double t[kPer];
+#pragma unroll
+          for (int u = 0; u < kPer; ++u) {
+            const int b = b0 + 32 * u;
+            t[u] = b < g.nb ? __ldcg(p + b) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kPer; ++u)
+            if (b0 + 32 * u < g.nb) sum = sum + t[u];
+        }
+        sum = warp_allsum(sum);
+        if (lane == 0) s_tot[m] = sum;
+      }
     }
   }
   if (lane == 0) s_ok = ok;

@@ -69,6 +69,9 @@ __device__ __forceinline__ bool allsum(double (&v)[NV], ClusterGroup& g, int) {
   return cluster_allsum<NV>(v, g);
 }
 
+// Doubles a cell the KEEP form holds in shared memory: x, r, aP, q.
+constexpr int kKeepArrays = 4;
+
 struct CgArgs {
   MeshDims d;
   SysF64 s;
@@ -89,13 +92,15 @@ struct CgArgs {
 // phase. Kernels pick them by their register budget. PF: threads 0..7 of the
 // block prefetch the block's next round of every streamed array into L2
 // (one bulk prefetch per array), for meshes whose working set exceeds L2.
-// KEEP: the thread's own cells' x, r, aP and this iteration's p and q stay
-// in the block's shared memory (`keep`, 5 x slice-length doubles) for the
-// whole solve: the update phase then reads no global memory, q is never
-// stored globally, and x goes back to global memory once, at the end. A
-// thread visits the same cells in both phases (and every iteration), so no
-// other thread ever reads what it keeps; the arithmetic and the order of
-// every sum are unchanged.
+// KEEP: the thread's own cells' x, r, aP and this iteration's q = A p stay
+// in the block's shared memory (`keep`, kKeepArrays x slice-length doubles)
+// for the whole solve: the update phase reads only the new direction from
+// global memory (the stencil phase stored it there for the neighbours), q
+// is never stored globally, and x goes back to global memory once, at the
+// end. A thread visits the same cells in both phases (and every iteration),
+// so no other thread ever reads what it keeps; the arithmetic and the order
+// of every sum are unchanged. The direction itself is not kept: the L1 room
+// it would take costs the stencil phase more than the update phase gains.
 template <bool SYM, int U, int UA, bool PF, class G, bool KEEP = false>
 __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
   const MeshDims& d = a.d;
@@ -105,8 +110,7 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
   double* __restrict__ kx = keep;
   double* __restrict__ kr = keep + (size_t)1 * (KEEP ? slen : 0);
   double* __restrict__ kd = keep + (size_t)2 * (KEEP ? slen : 0);
-  double* __restrict__ kp = keep + (size_t)3 * (KEEP ? slen : 0);
-  double* __restrict__ kq = keep + (size_t)4 * (KEEP ? slen : 0);
+  double* __restrict__ kq = keep + (size_t)3 * (KEEP ? slen : 0);
   const Coefs<double> A = coefs_of<double>(s.aP, s.aE, s.aN, s.aT, s.aW, s.aS, s.aB);
   const double* __restrict__ aP = s.aP;
   const double* __restrict__ b = s.b;
@@ -141,7 +145,6 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
           kx[o] = x[c0 + u * B];
           kr[o] = rv[u];
           kd[o] = dv[u];
-          kp[o] = zv;
         }
         v3[0] = v3[0] + (live ? bv[u] * bv[u] : 0.0);
         v3[1] = v3[1] + (live ? rv[u] * rv[u] : 0.0);
@@ -219,7 +222,6 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
             if (live) {
               pcur[c0 + u * B] = pc[u];
               if (KEEP) {
-                kp[c0 + u * B - own.begin] = pc[u];
                 kq[c0 + u * B - own.begin] = qv[u];
               } else {
                 q[c0 + u * B] = qv[u];
@@ -247,7 +249,7 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
           const int c = min(c0 + u * B, last);
           if (KEEP) {
             const int o = c - own.begin;
-            pv[u] = kp[o];
+            pv[u] = pcur[c];
             qv[u] = kq[o];
             dv[u] = kd[o];
             xv[u] = kx[o];
@@ -1294,7 +1296,7 @@ static const void* cg_keep_kernel_ptr(int block) {
 
 size_t keep_smem_bytes(long long n, int grid) {
   const long long chunk = (n + grid - 1) / grid;
-  return (size_t)chunk * 5 * sizeof(double);
+  return (size_t)chunk * kKeepArrays * sizeof(double);
 }
 
 int keep_max_coresident(int block, long long n, int grid, int sms) {

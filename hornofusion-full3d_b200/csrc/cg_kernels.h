@@ -93,8 +93,8 @@ cudaError_t launch_cg_f64_stream(const MeshDims& d, const SysF64& s, const Group
                                  int block, cudaStream_t st);
 int stream_stages(int block, int nr);
 int stream_max_coresident(int block, int nr, int sms);
-// The same solver with each block's own cells' x, r, aP, p and q kept in
-// its shared memory for the whole solve (5 doubles a cell, dynamic shared
+// The same solver with each block's own cells' x, r, aP and q kept in its
+// shared memory for the whole solve (4 doubles a cell, dynamic shared
 // memory of keep_smem_bytes); bit-identical to cg_f64_kernel on the same
 // launch. keep_max_coresident: blocks of that launch the device can hold at
 // once (0: the slice does not fit).

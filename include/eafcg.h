@@ -174,11 +174,12 @@ int eaf_cg_set_resident(eaf_cg_t h, int resident);
  * (the cluster all-reduce with clusters of one block) instead of an arrival
  * counter; same association, so the same bits as EAF_CG_KERNEL_LOADS */
 #define EAF_CG_KERNEL_SLOTS 3
-/* per-thread loads, with each block's own cells' x, r, aP, search direction
- * and A p kept in its shared memory for the whole solve, so the update phase
- * reads no global memory; same arithmetic in the same order, so the same
- * bits as EAF_CG_KERNEL_LOADS. Runs where a block's slice fits (5 doubles a
- * cell, about 5,000 cells a block), else the per-thread-load kernel does. */
+/* per-thread loads, with each block's own cells' x, r, aP and A p kept in
+ * its shared memory for the whole solve, so the update phase reads only the
+ * search direction from global memory; same arithmetic in the same order,
+ * so the same bits as EAF_CG_KERNEL_LOADS. Runs where a block's slice fits
+ * (4 doubles a cell, about 7,000 cells a block), else the per-thread-load
+ * kernel does. */
 #define EAF_CG_KERNEL_KEEP 4
 int eaf_cg_set_kernel(eaf_cg_t h, int kernel);
 int eaf_cg_last_kernel(eaf_cg_t h, int* kernel);
