@@ -749,6 +749,7 @@ def run_pstep(args):
             _, cres, nit, _ = cg.pressure_step(d, alpha_p, max_iter, tol, device_ptrs=True)
             kms += cg.last_timing()["kernel_ms"]
             iters.append(nit)
+        cg_kernel = solver_kernel_name(cg, cg.last_launch())
         e2e = 0.0
         h = _pinned_fields(eaf, f0)
         for _ in range(args.steps):
@@ -784,7 +785,7 @@ def run_pstep(args):
                         "algorithmic_bytes": "120 B per cell-iteration (CG) + 364 B per halo "
                                              "element (assembly) + 300 B per cell "
                                              "(corrections)",
-                        "kernel": "asm_* + cg_f64_kernel + pcorr_*"}
+                        "kernel": f"asm_* + {cg_kernel} + pcorr_*"}
     line["e2e"] = {"value": 1e3 / (e2e / args.steps), "unit": "steps/s",
                    "h2d_bytes_per_step": 24 * 8 * nh + 4 * 4 * nh + 8 * (nr + nth + nz + 12),
                    "d2h_bytes_per_step": 18 * 8 * nh + 3 * 4 * nh + 7 * 8 * nh}

@@ -94,13 +94,14 @@ struct CgArgs {
 // (one bulk prefetch per array), for meshes whose working set exceeds L2.
 // KEEP: the thread's own cells' x, r, aP and this iteration's q = A p stay
 // in the block's shared memory (`keep`, kKeepArrays x slice-length doubles)
-// for the whole solve: the update phase reads only the new direction from
-// global memory (the stencil phase stored it there for the neighbours), q
-// is never stored globally, and x goes back to global memory once, at the
-// end. A thread visits the same cells in both phases (and every iteration),
-// so no other thread ever reads what it keeps; the arithmetic and the order
-// of every sum are unchanged. The direction itself is not kept: the L1 room
-// it would take costs the stencil phase more than the update phase gains.
+// for the whole solve: the stencil takes the cell's own aP from there, the
+// update phase reads only the new direction from global memory (the
+// stencil phase stored it there for the neighbours), q is never stored
+// globally, and x goes back to global memory once, at the end. A thread
+// visits the same cells in both phases (and every iteration), so no other
+// thread ever reads what it keeps; the arithmetic and the order of every
+// sum are unchanged. The direction itself is not kept: the L1 room it
+// would take costs the stencil phase more than the update phase gains.
 template <bool SYM, int U, int UA, bool PF, class G, bool KEEP = false>
 __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
   const MeshDims& d = a.d;
@@ -185,7 +186,9 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
           for (int u = 0; u < UA; ++u) {
             const int c = min(c0 + u * B, last);
             pc[u] = pcur[c];
-            qv[u] = apply_row<SYM, double>(d, A, pcur, c);
+            qv[u] = KEEP ? apply_row_diag<SYM, double>(d, A, kd[c - own.begin], pc[u],
+                                                       [pcur](int cc) { return pcur[cc]; }, c)
+                         : apply_row<SYM, double>(d, A, pcur, c);
           }
 #pragma unroll
           for (int u = 0; u < UA; ++u) {
@@ -214,7 +217,8 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
           for (int u = 0; u < UA; ++u) {
             const int c = min(c0 + u * B, last);
             pc[u] = pnew(c);
-            qv[u] = apply_row_with<SYM, double>(d, A, pc[u], pnew, c);
+            qv[u] = KEEP ? apply_row_diag<SYM, double>(d, A, kd[c - own.begin], pc[u], pnew, c)
+                         : apply_row_with<SYM, double>(d, A, pc[u], pnew, c);
           }
 #pragma unroll
           for (int u = 0; u < UA; ++u) {

@@ -24,14 +24,15 @@ struct Coefs {
 // aN(south of c) and aB(c) = aT(c-plane); the wall links of a symmetric
 // operator are zero and the reference's Krylov vectors are zero in their r/z
 // halos, so the wall terms skipped here are exact zeros there too.
+// apply_row_diag: the same row with the cell's own aP given by the caller.
 template <bool SYM, typename T, typename XF>
-__device__ __forceinline__ T apply_row_with(const MeshDims& d, const Coefs<T>& A, T xc,
+__device__ __forceinline__ T apply_row_diag(const MeshDims& d, const Coefs<T>& A, T ap, T xc,
                                             XF xv, int c) {
   int i, j, k;
   cell_ijk(d, c, i, j, k);
   const int cs = j > 0 ? c - d.nr : c + (d.nth - 1) * d.nr;
   const int cn = j < d.nth - 1 ? c + d.nr : c - (d.nth - 1) * d.nr;
-  T y = A.aP[c] * xc;
+  T y = ap * xc;
   if (SYM) {
     if (i > 0) y = y - A.aE[c - 1] * xv(c - 1);
     if (i < d.nr - 1) y = y - A.aE[c] * xv(c + 1);
@@ -52,6 +53,12 @@ __device__ __forceinline__ T apply_row_with(const MeshDims& d, const Coefs<T>& A
     y = y - A.aT[c] * xt;
   }
   return y;
+}
+
+template <bool SYM, typename T, typename XF>
+__device__ __forceinline__ T apply_row_with(const MeshDims& d, const Coefs<T>& A, T xc,
+                                            XF xv, int c) {
+  return apply_row_diag<SYM, T>(d, A, A.aP[c], xc, xv, c);
 }
 
 // The operator applied to a stored vector x.
