@@ -99,6 +99,11 @@ static int max_coresident(const void* kernel, int block, int sms) {
 
 namespace eaf {
 
+std::mutex& launch_attr_mutex() {
+  static std::mutex m;
+  return m;
+}
+
 // Launch shape for a persistent kernel over n cells: an explicit
 // eaf_cg_set_launch shape, else the tuned shape of this mesh (FP64 solver),
 // else, for the reference-form FP64 solver on a mesh that fits, one

@@ -421,6 +421,7 @@ bool dsm_can_launch(long long n, int block, int cluster) {
   const int chunk = (int)((n + cluster - 1) / cluster);
   const size_t smem = dsm_smem_bytes(chunk);
   const void* k = (const void*)cg_dsm_kernel<false>;
+  std::lock_guard<std::mutex> attr_lock(launch_attr_mutex());
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
           cudaSuccess ||
       (cluster > 8 &&
@@ -466,6 +467,7 @@ cudaError_t launch_cg_f64_dsm(const MeshDims& d, const SysF64& s, const GroupWs&
   const size_t smem = dsm_smem_bytes(a.chunk);
   const void* k = signal == kDsmSignalMbarrier ? (const void*)cg_dsm_kernel<true>
                                                 : (const void*)cg_dsm_kernel<false>;
+  std::lock_guard<std::mutex> attr_lock(launch_attr_mutex());
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);

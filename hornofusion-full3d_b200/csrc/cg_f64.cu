@@ -71,6 +71,10 @@ __device__ __forceinline__ bool allsum(double (&v)[NV], ClusterGroup& g, int) {
 
 // Doubles a cell the KEEP form holds in shared memory: x, r, aP, q.
 constexpr int kKeepArrays = 4;
+// Partial-table slots of the flat solver: 0-2 the preamble's sums, 3 p.q in
+// the counter form, 4-5 r.r and r.z, 6-7 the two p.q slot sets of
+// group_allsum_slots (the table holds 8 doubles per block).
+constexpr int kPqSlotOffset = 6;
 
 struct CgArgs {
   MeshDims d;
@@ -102,7 +106,10 @@ struct CgArgs {
 // thread ever reads what it keeps; the arithmetic and the order of every
 // sum are unchanged. The direction itself is not kept: the L1 room it
 // would take costs the stencil phase more than the update phase gains.
-template <bool SYM, int U, int UA, bool PF, class G, bool KEEP = false>
+// PQS: the p.q all-reduce of a flat grid (Group) runs without a release,
+// through the slot sets at part + kPqSlotOffset * nb (group_allsum_slots),
+// up to 32 * kPerLane blocks; larger grids use the counter form.
+template <bool SYM, int U, int UA, bool PF, class G, bool KEEP = false, bool PQS = false>
 __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
   const MeshDims& d = a.d;
   const SysF64& s = a.s;
@@ -235,7 +242,14 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
           }
         }
       }
-      if (!(ok = allsum<1>(v1, g, 3))) break;
+      if constexpr (PQS) {
+        ok = g.nb <= 32 * kPerLane
+                 ? group_allsum_slots(v1, g, a.ws.part + (size_t)kPqSlotOffset * g.nb, iter)
+                 : allsum<1>(v1, g, 3);
+      } else {
+        ok = allsum<1>(v1, g, 3);
+      }
+      if (!ok) break;
       const double pq = v1[0];
       if (fabs(pq) < kSmall) break;
       const double alpha = rz / pq;
@@ -336,14 +350,18 @@ __global__ void __launch_bounds__(MAXB, 1) cg_f64_kernel(CgArgs a) {
   g.bid = blockIdx.x;
   g.timeout_ns = a.timeout_ns;
   g.epoch = 0;
+  // The fence-free p.q all-reduce is for the L2-resident meshes; beyond L2
+  // (PF) it measured slower (121.4 against 117.9 us per iteration at
+  // 120x240x168).
   if (*a.s.asym == 0)
-    cg_body<true, U, UA, PF>(a, g);
+    cg_body<true, U, UA, PF, Group, false, !PF>(a, g);
   else
-    cg_body<false, U, UA, PF>(a, g);
+    cg_body<false, U, UA, PF, Group, false, !PF>(a, g);
 }
 
 // The same solver with the own cells' update operands kept in shared memory
-// (cg_body's KEEP); blocks own at most kKeepMaxSlice cells.
+// (cg_body's KEEP); the launcher sizes the dynamic shared memory for the
+// largest slice.
 template <int MAXB, int U, int UA>
 __global__ void __launch_bounds__(MAXB, 1) cg_keep_kernel(CgArgs a) {
   extern __shared__ __align__(16) double keep_smem[];
@@ -357,9 +375,9 @@ __global__ void __launch_bounds__(MAXB, 1) cg_keep_kernel(CgArgs a) {
   g.timeout_ns = a.timeout_ns;
   g.epoch = 0;
   if (*a.s.asym == 0)
-    cg_body<true, U, UA, false, Group, true>(a, g, keep_smem);
+    cg_body<true, U, UA, false, Group, true, true>(a, g, keep_smem);
   else
-    cg_body<false, U, UA, false, Group, true>(a, g, keep_smem);
+    cg_body<false, U, UA, false, Group, true, true>(a, g, keep_smem);
 }
 
 // The same solver on a grid of thread-block clusters (cluster_red.cuh): the
@@ -1108,6 +1126,15 @@ cudaError_t launch_unpack_f64(const MeshDims& d, const double* x, double* phi,
   return cudaGetLastError();
 }
 
+// The two p.q slot sets of a flat launch of `grid` blocks, filled with the
+// empty-slot marker (group_allsum_slots).
+static cudaError_t fill_pq_slots(const GroupWs& ws, int grid, cudaStream_t st) {
+  // (harmless where the kernel keeps the counter form for p.q)
+  if (grid <= 1 || grid > 32 * kPerLane) return cudaSuccess;
+  fill_marker_kernel<<<1, 320, 0, st>>>(ws.part + (size_t)kPqSlotOffset * grid, 2 * grid);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
                           int max_iter, double tol, uint64_t timeout_ns, int grid,
                           int block, cudaStream_t st) {
@@ -1120,6 +1147,7 @@ cudaError_t launch_cg_f64(const MeshDims& d, const SysF64& s, const GroupWs& ws,
   a.timeout_ns = timeout_ns;
   cudaError_t e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = fill_pq_slots(ws, grid, st);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
   return cudaLaunchCooperativeKernel(cg_f64_kernel_ptr(block, d.n), dim3(grid),
@@ -1259,6 +1287,7 @@ int stream_max_coresident(int block, int nr, int sms) {
   if (S < 2) return 0;
   const void* k = cg_stream_kernel_ptr(block);
   const size_t smem = (size_t)stream_layout(block, nr, S).stage * 8 * S;
+  std::lock_guard<std::mutex> attr_lock(launch_attr_mutex());
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return 0;
@@ -1282,6 +1311,7 @@ cudaError_t launch_cg_f64_stream(const MeshDims& d, const SysF64& s, const Group
   a.timeout_ns = timeout_ns;
   const void* k = cg_stream_kernel_ptr(block);
   const size_t smem = (size_t)stream_layout(block, d.nr, S).stage * 8 * S;
+  std::lock_guard<std::mutex> attr_lock(launch_attr_mutex());
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
@@ -1312,6 +1342,7 @@ int keep_max_coresident(int block, long long n, int grid, int sms) {
   const size_t smem = keep_smem_bytes(n, grid);
   if (smem + 8 * 1024 > (size_t)optin) return 0;  // static shared memory and slack
   const void* k = cg_keep_kernel_ptr(block);
+  std::lock_guard<std::mutex> attr_lock(launch_attr_mutex());
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess) {
     (void)cudaGetLastError();
@@ -1337,10 +1368,12 @@ cudaError_t launch_cg_f64_keep(const MeshDims& d, const SysF64& s, const GroupWs
   a.timeout_ns = timeout_ns;
   const void* k = cg_keep_kernel_ptr(block);
   const size_t smem = keep_smem_bytes(d.n, grid);
+  std::lock_guard<std::mutex> attr_lock(launch_attr_mutex());
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = fill_pq_slots(ws, grid, st);
   if (e != cudaSuccess) return e;
   void* args[] = {&a};
   return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(block), args, smem, st);

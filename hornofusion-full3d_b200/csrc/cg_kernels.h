@@ -5,10 +5,19 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "cg_common.cuh"
 #include "eafcg.h"
 
 namespace eaf {
+
+// Held around "set a kernel's dynamic shared memory size, then launch it or
+// query its occupancy": the size is an attribute of the function, so two
+// host threads (a server's worker and a caller's solve) that launch one
+// kernel with different sizes must not interleave the two steps.
+std::mutex& launch_attr_mutex();
+
 
 // Written by the solver kernel (block 0, thread 0) at the end of a solve.
 struct SolveResult {

@@ -153,6 +153,135 @@ static __device__ __forceinline__ ClusterSmem& cluster_smem() {
   return s;
 }
 
+// ---------------------------------------------------------------------------
+// One-sum group all-reduce without a release, for the flat solver's p.q.
+// Nothing a block writes in the stencil phase is read by another block before
+// the r.r / r.z all-reduce that follows the update phase, and that one keeps
+// its release and acquire; so this all-reduce only has to carry the partials,
+// and its cost is no longer a release that waits for the SM's outstanding
+// stores. Each block's warp 0 folds its partial as group_allsum_w0 does, then
+// lane 0 writes it with a relaxed store into its slot of the set of this
+// iteration and adds 1 to the group counter with a relaxed add (a doorbell,
+// no ordering). Lane 0 polls the counter (relaxed) up to the all-reduce's
+// target; then every lane loads its slots (blocks l, l+32, ...) with relaxed
+// loads, re-loading any that still holds the marker (the value is the
+// signal: a signalling NaN no arithmetic produces), and the partials are
+// folded in group_allsum_w0's order, so the totals are bit-identical to it.
+//
+// Slots: two sets of nb doubles at `slots` (set = iteration & 1), filled
+// with the marker before the launch. At iteration i a block first resets its
+// slot of the other set, last written at i - 1: every block read that set
+// before it arrived at the r.r / r.z all-reduce of iteration i - 1, whose
+// release/acquire orders those reads before this reset, and the same
+// all-reduce of iteration i orders the reset before the reads of iteration
+// i + 1. Counter epochs are shared with group_allsum_w0: every block adds 1
+// per all-reduce, so the count reaches epoch * nb only when all have.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void red_relaxed_add_u64(unsigned long long* p,
+                                                    unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ bool group_allsum_slots(double (&v)[1], Group& g, double* slots,
+                                                   int iter) {
+  __shared__ double s_w[32];
+  __shared__ double s_tot;
+  __shared__ int s_ok;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nthreads = blockDim.x;
+  v[0] = warp_allsum(v[0]);
+  if (w != 0) {
+    if (lane == 0) s_w[w] = v[0];
+    named_arrive(kBarPosted, nthreads);
+    named_sync(kBarTotal, nthreads);
+    v[0] = s_tot;
+    return s_ok != 0;
+  }
+  if (lane == 0) s_w[0] = v[0];
+  named_sync(kBarPosted, nthreads);
+  const int nw = (nthreads + 31) >> 5;
+  const double blk = warp_allsum(lane < nw ? s_w[lane] : 0.0);
+  int ok = 1;
+  if (g.nb == 1) {
+    if (lane == 0) s_tot = blk;
+  } else {
+    g.epoch = __shfl_sync(0xffffffffu, g.epoch, 0) + 1;
+    const unsigned long long target = g.epoch * (unsigned long long)g.nb;
+    double* cur = slots + (size_t)(iter & 1) * g.nb;
+    double* other = slots + (size_t)((iter + 1) & 1) * g.nb;
+    if (lane == 0) {
+      st_relaxed_f64(other + g.bid, __longlong_as_double((long long)kSlotMarker));
+      st_relaxed_f64(cur + g.bid, blk);
+      red_relaxed_add_u64(g.counter, 1ull);
+      uint64_t t0 = 0;
+      uint32_t spins = 0;
+      while (ld_relaxed_u64(g.counter) < target) {
+        if ((++spins & 63u) == 0) {
+          if (spins == 64u) t0 = global_ns();
+          if (ld_volatile_i32(g.err) != 0) { ok = 0; break; }
+          if (global_ns() - t0 > g.timeout_ns) {
+            atomicCAS(g.err, 0, (int)EAF_ETIMEOUT);
+            ok = 0;
+            break;
+          }
+        }
+      }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    double sum = 0.0;
+    if (ok) {
+      double t[kPerLane];
+#pragma unroll
+      for (int u = 0; u < kPerLane; ++u) {
+        const int b = lane + 32 * u;
+        t[u] = b < g.nb ? ld_relaxed_f64(cur + b) : 0.0;
+      }
+      // A partial whose doorbell overtook it: load it again (bounded).
+      uint64_t t0 = 0;
+      uint32_t spins = 0;
+      bool mine = true;
+#pragma unroll
+      for (int u = 0; u < kPerLane; ++u) mine = mine && !is_marker(t[u]);
+      while (!__all_sync(0xffffffffu, mine)) {
+#pragma unroll
+        for (int u = 0; u < kPerLane; ++u) {
+          const int b = lane + 32 * u;
+          if (is_marker(t[u])) t[u] = ld_relaxed_f64(cur + b);
+        }
+        mine = true;
+#pragma unroll
+        for (int u = 0; u < kPerLane; ++u) mine = mine && !is_marker(t[u]);
+        if ((++spins & 15u) == 0) {
+          if (spins == 16u) t0 = global_ns();
+          int bad = 0;
+          if (lane == 0) {
+            if (ld_volatile_i32(g.err) != 0) {
+              bad = 1;
+            } else if (global_ns() - t0 > g.timeout_ns) {
+              atomicCAS(g.err, 0, (int)EAF_ETIMEOUT);
+              bad = 1;
+            }
+          }
+          if (__shfl_sync(0xffffffffu, bad, 0)) {
+            ok = 0;
+            break;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kPerLane; ++u)
+        if (lane + 32 * u < g.nb) sum = sum + t[u];
+    }
+    sum = warp_allsum(sum);
+    if (lane == 0) s_tot = sum;
+  }
+  if (lane == 0) s_ok = ok;
+  named_arrive(kBarTotal, nthreads);
+  __syncwarp();
+  v[0] = s_tot;
+  return ok != 0;
+}
+
 template <int NV, typename T>
 __device__ __forceinline__ bool cluster_allsum(T (&v)[NV], ClusterGroup& g) {
   static_assert(NV <= kClusterSlotsNV, "too many sums for one cluster all-reduce");

@@ -571,6 +571,7 @@ cudaError_t launch_tdma_f64(const HaloInputs& in, double* phi, int nr, int nth, 
   a.timeout_ns = timeout_ns;
   const int grid = tdma_grid(nr, nth, nz);
   const size_t smem = (size_t)(2 * kBufArrays + 3) * lmax * sizeof(double);
+  std::lock_guard<std::mutex> attr_lock(launch_attr_mutex());
   cudaError_t e = cudaSuccess;
   if (smem > 48 * 1024)
     e = cudaFuncSetAttribute((const void*)tdma_kernel,

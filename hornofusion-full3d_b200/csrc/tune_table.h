@@ -35,7 +35,7 @@ struct TunedLaunch {
 static constexpr TunedLaunch kTunedLaunches[] = {
     {12, 24, 16, 288, 16, 16, 0},
     {18, 36, 24, 512, 16, 16, 0},
-    {35, 70, 50, 512, 120, 1, 2},
+    {35, 70, 50, 512, 148, 1, 2},
     {60, 120, 84, 512, 148, 1, 2},
     {120, 240, 168, 1024, 148, 1, 0},
 };

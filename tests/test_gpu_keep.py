@@ -126,3 +126,39 @@ def test_warm_started_repeat_solves_on_one_handle():
             assert cg.last_kernel() == cg.KERNEL_KEEP
             ro, no = oracle.cg(s, ref, 60, 0.0, plan=(148, 512))
             assert (res, nit) == (ro, no) and np.array_equal(phi, ref), k
+
+
+def test_concurrent_solves_on_two_host_threads():
+    """Two host threads solving different meshes at once through the kept
+    form (different dynamic shared-memory sizes of one kernel) get the bits
+    each gets alone: the size attribute and the launch are taken together."""
+    import threading
+    eaf = pkg()
+    g = gen()
+    cases = [(g.make_system(*g.PRODUCTION, seed=6), 120), (g.make_system(35, 70, 50, 16, seed=7), 200)]
+
+    def run(s, iters, out):
+        phi = g.zeros_phi(s.nr, s.nth, s.nz)
+        with eaf.CGSolver(s.nr, s.nth, s.nz) as cg:
+            for _ in range(6):
+                phi[...] = 0.0
+                res, nit, st = cg.solve(s.arrays(), phi, iters, 0.0)
+                out.append((res, nit, st, cg.last_kernel(), phi.copy()))
+
+    alone = []
+    for s, iters in cases:
+        o = []
+        run(s, iters, o)
+        alone.append(o[0])
+    outs = [[], []]
+    threads = [threading.Thread(target=run, args=(s, iters, outs[i]))
+               for i, (s, iters) in enumerate(cases)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for i in range(2):
+        assert len(outs[i]) == 6
+        for res, nit, st, kern, phi in outs[i]:
+            assert kern == eaf.CGSolver.KERNEL_KEEP
+            assert (res, nit, st) == alone[i][:3] and np.array_equal(phi, alone[i][4])
