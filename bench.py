@@ -376,7 +376,10 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_ci / (e2e_ms / 1e3), "unit": "cell-iters/s",
                 "h2d_bytes_per_step": 9 * halo_bytes,
                 "d2h_bytes_per_step": halo_bytes + 40},
-        "gpu_launches": 3 * args.steps,
+        # pack, solver, unpack; the flat kernels' launcher also fills the
+        # p.q slot sets with the empty-slot marker (one small kernel)
+        "gpu_launches": (4 if kernel in ("cg_keep_kernel", "cg_f64_kernel")
+                         and 1 < plan[0] <= 160 else 3) * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -795,7 +798,9 @@ def run_pstep(args):
                             "kind": "port",
                             "sample": f"oracle port: assembly and corrections on one thread, "
                                       f"CG on {cores} threads, one step, {cpu_s:.2f} s"}
-    line["gpu_launches"] = (4 + 3 + 3) * args.steps
+    # assembly 4; pack, solver, unpack (+ the p.q slot fill of a flat grid); corrections 3
+    cg_launches = 4 if cg_kernel in ("cg_keep_kernel", "cg_f64_kernel") else 3
+    line["gpu_launches"] = (4 + cg_launches + 3) * args.steps
     print(json.dumps(line), flush=True)
     return 0
 
