@@ -162,3 +162,17 @@ def test_concurrent_solves_on_two_host_threads():
         for res, nit, st, kern, phi in outs[i]:
             assert kern == eaf.CGSolver.KERNEL_KEEP
             assert (res, nit, st) == alone[i][:3] and np.array_equal(phi, alone[i][4])
+
+
+@pytest.mark.parametrize("dims,block,grid,iters,tol", [
+    ((60, 120, 84, 24), 64, 296, 150, 0.0),     # more blocks than the p.q slot form takes
+    ((12, 24, 16, 8), 256, 1, 100000, TOL),     # one block: no group stage at all
+    ((18, 36, 24, 8), 128, 160, 100000, TOL)])  # the slot form's largest grid
+def test_grid_sizes_around_the_slot_all_reduce(dims, block, grid, iters, tol):
+    """The p.q all-reduce without a release runs on flat grids of 2 to 160
+    blocks; one block needs no group stage and larger grids keep the counter
+    form. All give the oracle's bits for their plan."""
+    g = gen()
+    s = g.make_system(*dims, seed=9)
+    res, nit, st, plan = assert_keep_bitwise(s, g.zeros_phi(*dims[:3]), iters, tol, block, grid)
+    assert plan == (grid, block) and st == 0
