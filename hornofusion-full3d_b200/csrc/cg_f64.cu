@@ -16,6 +16,14 @@
 //      partial r.r and r.z                         -> all-reduce (r.r, r.z)
 // The scalar recurrences (alpha, beta, residual, exit tests) are evaluated
 // redundantly and bit-identically by every block.
+//
+// Forms: cg_f64_kernel (per-thread loads), cg_keep_kernel (the same with
+// each block's own cells' x, r, aP and q kept in shared memory for the whole
+// solve), cg_stream_kernel (operands staged by bulk copies), cg_cluster_kernel
+// (grid of thread-block clusters), cg1_f64_kernel (one all-reduce per
+// iteration, rearranged recurrences) and batch_f64_kernel (many systems on
+// lanes of one launch). On flat grids of up to 160 blocks the p.q all-reduce
+// carries no release (group_allsum_slots in cluster_red.cuh).
 #include <math.h>
 
 #include "cg_kernels.h"

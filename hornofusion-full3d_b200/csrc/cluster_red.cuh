@@ -1,7 +1,11 @@
-// Cluster all-reduce: the grid of a persistent solver launched as clusters of
-// C co-scheduled blocks (thread-block clusters, up to 16 per cluster), with
-// the group reduction split into a distributed-shared-memory stage inside
-// each cluster and a global stage among the cluster leaders only.
+// Slot-signalled all-reduces (the value in a slot is its own signal: slots
+// hold a signalling-NaN marker until written):
+//   * cluster_allsum: the grid of a persistent solver launched as clusters of
+//     C co-scheduled blocks (thread-block clusters, up to 16 per cluster),
+//     with the group reduction split into a distributed-shared-memory stage
+//     inside each cluster and a global stage among the cluster leaders only;
+//   * group_allsum_slots (further below): the flat grid's p.q all-reduce
+//     without a release.
 //
 //   1. every block folds its partial as the group all-reduce does (warp
 //      butterflies, warp 0 folds the warp sums) and warp 0 writes it into the
