@@ -566,3 +566,10 @@ def host_empty(shape, dtype=np.float64) -> np.ndarray:
 
 def barrier_timeout_selftest(device: int = 0, timeout_ms: float = 20.0) -> int:
     return load().eaf_selftest_barrier_timeout(device, float(timeout_ms))
+
+
+def allreduce_timeout_selftest(device: int = 0, timeout_ms: float = 20.0, mode: int = 0) -> int:
+    """The release-free p.q all-reduce's bounded waits (mode 0: the arrival
+    count never completes; mode 1: a partial is never written) must give
+    EAF_ETIMEOUT."""
+    return load().eaf_selftest_allreduce_timeout(device, float(timeout_ms), int(mode))

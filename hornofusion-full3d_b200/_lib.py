@@ -139,6 +139,7 @@ SIGNATURES = [
     ("eaf_host_register", _ci, [_vp, _sz]),
     ("eaf_host_unregister", _ci, [_vp]),
     ("eaf_selftest_barrier_timeout", _ci, [_ci, _cd]),
+    ("eaf_selftest_allreduce_timeout", _ci, [_ci, _cd, _ci]),
     ("eaf_diag_allreduce_us", _ci, [_ci, _ci, _ci, _ci, _ci, _pd]),
     ("eaf_diag_div_check", _ci, [_ci, ctypes.c_longlong, ctypes.c_ulonglong,
                                  ctypes.POINTER(ctypes.c_longlong),

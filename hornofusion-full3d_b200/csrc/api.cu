@@ -667,6 +667,34 @@ int eaf_selftest_barrier_timeout(int device, double timeout_ms) {
   return err_h;
 }
 
+int eaf_selftest_allreduce_timeout(int device, double timeout_ms, int mode) {
+  if (!(timeout_ms > 0.0) || timeout_ms > 10000.0 || (mode != 0 && mode != 1))
+    return EAF_EINVAL;
+  eaf::DeviceGuard guard(device);
+  if (!guard.ok()) return EAF_ECUDA;
+  GroupWs ws = {};
+  cudaStream_t st = nullptr;
+  int err_h = 0;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ws.part, sizeof(double) * 16);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ws.counter, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ws.err, sizeof(int));
+  if (e == cudaSuccess)
+    e = eaf::launch_allreduce_selftest(ws, (uint64_t)(timeout_ms * 1.0e6), mode, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&err_h, ws.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(ws.part);
+  cudaFree(ws.counter);
+  cudaFree(ws.err);
+  if (st) cudaStreamDestroy(st);
+  if (e != cudaSuccess) {
+    set_error("selftest", e);
+    return EAF_ECUDA;
+  }
+  return err_h;
+}
+
 }  // extern "C"
 
 namespace eaf {

@@ -1134,6 +1134,44 @@ cudaError_t launch_unpack_f64(const MeshDims& d, const double* x, double* phi,
   return cudaGetLastError();
 }
 
+// Self-test of group_allsum_slots' bounded waits. mode 0: two blocks of a
+// group declared with three members (the third never arrives, so the count
+// never completes); mode 1: one block of a group of two, the count preset to
+// one arrival, the other block's slot left holding the marker (its partial
+// never comes). Every wait expires and the kernel reports EAF_ETIMEOUT.
+__global__ void allreduce_selftest_kernel(GroupWs ws, uint64_t timeout_ns, int mode) {
+  Group g;
+  g.counter = ws.counter;
+  g.err = ws.err;
+  g.part = ws.part;
+  g.stage = group_stage_smem();
+  g.nb = mode == 0 ? 3 : 2;
+  g.bid = blockIdx.x;
+  g.timeout_ns = timeout_ns;
+  g.epoch = 0;
+  double v[1] = {1.0};
+  group_allsum_slots(v, g, ws.part, 1);
+}
+
+cudaError_t launch_allreduce_selftest(const GroupWs& ws, uint64_t timeout_ns, int mode,
+                                      cudaStream_t st) {
+  if (mode != 0 && mode != 1) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(ws.counter, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess && mode == 1) {
+    const unsigned long long one = 1;
+    e = cudaMemcpyAsync(ws.counter, &one, sizeof(one), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // `one` lives on this frame
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  fill_marker_kernel<<<1, 32, 0, st>>>(ws.part, 16);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&ws, (void*)&timeout_ns, (void*)&mode};
+  return cudaLaunchCooperativeKernel((const void*)allreduce_selftest_kernel,
+                                     dim3(mode == 0 ? 2 : 1), dim3(64), args, 0, st);
+}
+
 // The two p.q slot sets of a flat launch of `grid` blocks, filled with the
 // empty-slot marker (group_allsum_slots).
 static cudaError_t fill_pq_slots(const GroupWs& ws, int grid, cudaStream_t st) {

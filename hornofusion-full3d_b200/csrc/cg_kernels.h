@@ -262,5 +262,9 @@ const void* batch_mixed_kernel_ptr();
 // Barrier self-test (api.cu).
 cudaError_t launch_barrier_selftest(const GroupWs& ws, uint64_t timeout_ns,
                                     cudaStream_t st);
+// Self-test of the release-free p.q all-reduce's waits (cg_f64.cu): ws.part
+// holds at least 16 doubles.
+cudaError_t launch_allreduce_selftest(const GroupWs& ws, uint64_t timeout_ns, int mode,
+                                      cudaStream_t st);
 
 }  // namespace eaf

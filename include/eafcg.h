@@ -541,6 +541,15 @@ int eaf_cg_solve_f64_noalloc(int nr, int nth, int nz, int device, void* stream,
  * intact. No reference counterpart (failure-detection test hook). */
 int eaf_selftest_barrier_timeout(int device, double timeout_ms);
 
+/* Self-test of the bounded waits of the flat solver's release-free p.q
+ * all-reduce. mode 0: two blocks of a group declared with three members,
+ * so the arrival count never completes; mode 1: one block of a group of two
+ * whose count is preset as if the other had arrived but whose slot is never
+ * written, so the re-load of the missing partial never succeeds. Either must
+ * return EAF_ETIMEOUT after about timeout_ms with the device context intact.
+ * No reference counterpart (failure-detection test hook). */
+int eaf_selftest_allreduce_timeout(int device, double timeout_ms, int mode);
+
 /* Diagnostics (no reference counterpart): checks, on n generated operand
  * pairs (random over a wide exponent range, exact and near-halfway
  * quotients, zeros, infinities, NaN), that the division the TDMA sweeps use

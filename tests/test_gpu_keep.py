@@ -176,3 +176,26 @@ def test_grid_sizes_around_the_slot_all_reduce(dims, block, grid, iters, tol):
     s = g.make_system(*dims, seed=9)
     res, nit, st, plan = assert_keep_bitwise(s, g.zeros_phi(*dims[:3]), iters, tol, block, grid)
     assert plan == (grid, block) and st == 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_release_free_all_reduce_waits_are_bounded(mode):
+    """The p.q all-reduce's two waits -- for the arrival count (mode 0: a
+    member never arrives) and for a partial whose doorbell came first (mode
+    1: the partial is never written) -- give up after their bound with
+    EAF_ETIMEOUT, and the context stays usable: a solve afterwards gives the
+    oracle's bits."""
+    import oracle
+    eaf = pkg()
+    g = gen()
+    assert eaf.allreduce_timeout_selftest(0, 20.0, mode) == eaf._lib.EAF_ETIMEOUT
+    s = g.make_system(*g.PRODUCTION, seed=2)
+    phi = g.zeros_phi(60, 120, 84)
+    with eaf.CGSolver(60, 120, 84) as cg:
+        cg.set_launch(512, 148)
+        cg.set_kernel(cg.KERNEL_KEEP)
+        res, nit, st = cg.solve(s.arrays(), phi, 50, 0.0)
+        assert cg.last_kernel() == cg.KERNEL_KEEP and st == 0
+    ref = g.zeros_phi(60, 120, 84)
+    assert oracle.cg(s, ref, 50, 0.0, plan=(148, 512)) == (res, nit)
+    assert np.array_equal(phi, ref)
