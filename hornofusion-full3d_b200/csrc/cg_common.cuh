@@ -95,6 +95,7 @@ struct Group {
   int bid;            // this block's index in the group
   uint64_t timeout_ns;
   unsigned long long epoch;  // barriers passed (meaningful in thread 0)
+  int pq_seq = 0;            // release-free p.q all-reduces passed (all threads)
 };
 
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {

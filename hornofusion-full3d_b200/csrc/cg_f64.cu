@@ -252,7 +252,7 @@ __device__ void cg_body(const CgArgs& a, G& g, double* keep = nullptr) {
       }
       if constexpr (PQS) {
         ok = g.nb <= 32 * kPerLane
-                 ? group_allsum_slots(v1, g, a.ws.part + (size_t)kPqSlotOffset * g.nb, iter)
+                 ? group_allsum_slots(v1, g, a.ws.part + (size_t)kPqSlotOffset * g.nb)
                  : allsum<1>(v1, g, 3);
       } else {
         ok = allsum<1>(v1, g, 3);
@@ -994,6 +994,9 @@ __global__ void __launch_bounds__(kBatchBlock, 2) batch_f64_kernel(BatchF64Args 
     ca.max_iter = a.max_iter;
     ca.tol = a.tol;
     ca.timeout_ns = a.timeout_ns;
+    // The lanes keep the counter form for p.q: many lanes polling without
+    // the release measured slower (157.0 against 161.7 solves/s on the
+    // 96-system mix).
     if (*bs.s.asym == 0)
       cg_body<true, 2, 1, false, Group>(ca, g);
     else
@@ -1150,7 +1153,7 @@ __global__ void allreduce_selftest_kernel(GroupWs ws, uint64_t timeout_ns, int m
   g.timeout_ns = timeout_ns;
   g.epoch = 0;
   double v[1] = {1.0};
-  group_allsum_slots(v, g, ws.part, 1);
+  group_allsum_slots(v, g, ws.part);
 }
 
 cudaError_t launch_allreduce_selftest(const GroupWs& ws, uint64_t timeout_ns, int mode,

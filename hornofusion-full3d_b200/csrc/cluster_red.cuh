@@ -172,22 +172,25 @@ static __device__ __forceinline__ ClusterSmem& cluster_smem() {
 // signal: a signalling NaN no arithmetic produces), and the partials are
 // folded in group_allsum_w0's order, so the totals are bit-identical to it.
 //
-// Slots: two sets of nb doubles at `slots` (set = iteration & 1), filled
-// with the marker before the launch. At iteration i a block first resets its
-// slot of the other set, last written at i - 1: every block read that set
-// before it arrived at the r.r / r.z all-reduce of iteration i - 1, whose
-// release/acquire orders those reads before this reset, and the same
-// all-reduce of iteration i orders the reset before the reads of iteration
-// i + 1. Counter epochs are shared with group_allsum_w0: every block adds 1
-// per all-reduce, so the count reaches epoch * nb only when all have.
+// Slots: two sets of nb doubles at `slots`, used alternately by the group's
+// successive p.q all-reduces (g.pq_seq counts them, so the alternation also
+// holds across several solves by one group), filled with the marker before
+// the launch. At its s-th p.q all-reduce a block first resets its slot of
+// the other set, last written at s - 1: every block read that set before it
+// arrived at the next all-reduce with a release (the r.r / r.z of the same
+// iteration, or the preamble of a following solve), whose release/acquire
+// orders those reads before this reset; the release/acquire all-reduce
+// between s and s + 1 orders the reset before the reads of s + 1.
+// Counter epochs are shared with group_allsum_w0: every block adds 1 per
+// all-reduce, so the count reaches epoch * nb only when all have.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void red_relaxed_add_u64(unsigned long long* p,
                                                     unsigned long long v) {
   asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ bool group_allsum_slots(double (&v)[1], Group& g, double* slots,
-                                                   int iter) {
+__device__ __forceinline__ bool group_allsum_slots(double (&v)[1], Group& g, double* slots) {
+  const int seq = ++g.pq_seq;
   __shared__ double s_w[32];
   __shared__ double s_tot;
   __shared__ int s_ok;
@@ -211,8 +214,8 @@ __device__ __forceinline__ bool group_allsum_slots(double (&v)[1], Group& g, dou
   } else {
     g.epoch = __shfl_sync(0xffffffffu, g.epoch, 0) + 1;
     const unsigned long long target = g.epoch * (unsigned long long)g.nb;
-    double* cur = slots + (size_t)(iter & 1) * g.nb;
-    double* other = slots + (size_t)((iter + 1) & 1) * g.nb;
+    double* cur = slots + (size_t)(seq & 1) * g.nb;
+    double* other = slots + (size_t)((seq + 1) & 1) * g.nb;
     if (lane == 0) {
       st_relaxed_f64(other + g.bid, __longlong_as_double((long long)kSlotMarker));
       st_relaxed_f64(cur + g.bid, blk);
